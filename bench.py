@@ -1,0 +1,336 @@
+"""Benchmark: rotations/s of the docking hot path at 128^3, 54,000 rotations.
+
+Workload: a synthetic receptor of 500 residues (~4,000 heavy atoms) and ligand
+of 250 residues (~1,900 atoms) (megadock_b200.synth, seed 1000), FFT N = 128,
+the 54,000-rotation set, top-3 poses per rotation.  One step = every rotation
+of that job through the device pipeline (rotate, voxelize, forward FFT,
+conj(R^) product, inverse FFT, top-t).
+
+  value   batched form (rotations per launch > 1, one CUDA graph), inputs
+          resident in HBM (rotation matrices and pose buffer on the device)
+  plain   the plain form (one rotation per fused pipeline) on the same GPU
+  e2e     the batched form through the C ABI with host buffers: receptor grid
+          upload + receptor FFT + ligand upload + md_dock (rotation matrices in,
+          poses out) every step
+  roofline  dominant kernel from per-stage CUDA events (md_dock_profile on the
+          launch stream), algorithmic bytes per launch / mean launch time
+  cpu_baseline  the reference's own CPU program (oracle/_ref/megadock-ref,
+          MEGADOCK CPU sources + project FFT shim) on this host, bounded sample
+
+--impl reference runs only the reference's CPU program on the same workload
+(bounded sample per step) and prints its line.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+N_FFT = 128
+N_REC, N_LIG, SEED = 500, 250, 1000
+T_POSES = 3
+ROT_SET = 54000
+METRIC = "rotations/sec at 128^3, 54k rot: batched vs plain fused, same GPU, 1e-4 tol"
+REF_SAMPLE_ROT = 360
+
+
+def _peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return d.get("hbm_gbs", 6650.0), "measured"
+    return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    def __init__(self, index=0):
+        self.index = index
+        self.rows = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def __enter__(self):
+        def run():
+            q = ("clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap,utilization.gpu")
+            try:
+                p = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                                      "--format=csv,noheader,nounits", "-lms", "200"],
+                                     stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            except OSError:
+                return
+            while not self._stop.is_set():
+                line = p.stdout.readline()
+                if not line:
+                    break
+                self.rows.append([x.strip() for x in line.split(",")])
+            p.terminate()
+
+        self._t = threading.Thread(target=run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        self._t.join(timeout=3)
+
+    def summary(self):
+        load = [r for r in self.rows if len(r) >= 7 and r[6].isdigit() and int(r[6]) > 50]
+        rows = load or self.rows
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm = [float(r[0]) for r in rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if len(r) > 2 + k and r[2 + k] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def make_inputs(tmp):
+    from megadock_b200 import synth
+    return synth.write_pair(tmp, N_REC, N_LIG, SEED, stem="bench")
+
+
+def cpu_reference(rp, lp, nrot=REF_SAMPLE_ROT):
+    """Time the reference's CPU program (all host cores) on nrot rotations."""
+    from oracle import ref
+    cores = os.cpu_count() or 1
+    env = dict(os.environ, OMP_NUM_THREADS=str(cores), MD_SHIM_FFT="fp32")
+    with tempfile.TemporaryDirectory() as d:
+        out = os.path.join(d, "ref.out")
+        res = subprocess.run([str(ref.REF_BIN), "-R", rp, "-L", lp, "-F", str(N_FFT), "-t", str(T_POSES), "-r",
+                              str(nrot), "-o", out], capture_output=True, text=True, env=env)
+    if res.returncode != 0:
+        raise RuntimeError(res.stderr[-500:])
+    m = re.search(r"CPU time \(docking\)\s*=\s*([0-9.]+)", res.stdout)
+    secs = float(m.group(1))
+    return nrot / secs, cores, secs
+
+
+def run_reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from oracle import ref
+    with tempfile.TemporaryDirectory() as tmp:
+        rp, lp = make_inputs(tmp)
+        if not ref.available():
+            print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref (reference compiled from its "
+                                                                  "sources) was not built on this machine"}))
+            return
+        for _ in range(args.warmup):
+            cpu_reference(rp, lp)
+        rates = []
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            r, cores, secs = cpu_reference(rp, lp)
+            rates.append(r)
+        wall = time.perf_counter() - t0
+    value = statistics.mean(rates)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "rotations/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * wall / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"plain docking, {N_REC}/{N_LIG}-residue synthetic pair, N={N_FFT}, t={T_POSES}, "
+                               f"sampled {REF_SAMPLE_ROT} of {ROT_SET} rotations per step",
+                   "fft": N_FFT, "rotations": ROT_SET, "t": T_POSES},
+        "cpu_baseline": {"value": value, "unit": "rotations/s", "cores": cores, "kind": "reference",
+                         "sample": f"{REF_SAMPLE_ROT} rotations per step (MEGADOCK CPU sources + FFTW-API shim, "
+                                   f"OpenMP over all host cores)"},
+        "e2e": {"value": value, "unit": "rotations/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--batch", type=int, default=0, help="rotations per launch (0 = autotune)")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference_arm(args)
+
+    import numpy as np
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    from megadock_b200 import FFTProcess, Job, rotation_matrices
+    from megadock_b200.tune import autotune_batch
+
+    # a dedicated stream: the library captures CUDA graphs on it, which the
+    # legacy default stream does not allow
+    stream = torch.cuda.Stream(device=local)
+    torch.cuda.set_stream(stream)
+    with tempfile.TemporaryDirectory() as tmp:
+        rp, lp = make_inputs(tmp)
+        job = Job(["-R", rp, "-L", lp, "-F", str(N_FFT), "-t", str(T_POSES), "-D", "-o",
+                   os.path.join(tmp, "bench.out")])
+        rr, ri = job.receptor_grids()
+        xyz, rad, q = job.ligand_atoms()
+        mats = rotation_matrices(job.rotation_angles())
+        nrot = len(mats)
+        fp = FFTProcess(local, stream=stream.cuda_stream)
+        fp.alloc_array(job.nf1, job.grid_width, job.grid_coord())
+        fp.receptor_fft(rr, ri)
+        fp.ligand_data_transfer_gpu(xyz, rad, q, job.lig_core)
+        d_rot = torch.from_numpy(mats).to(f"cuda:{local}")
+        d_pose = torch.zeros(nrot * T_POSES * 5, dtype=torch.int32, device=f"cuda:{local}")
+
+        batch = args.batch or autotune_batch(fp, d_rot.data_ptr(), d_pose.data_ptr(), T_POSES)
+
+        def timed(fn, steps, warmup):
+            for _ in range(warmup):
+                fn()
+            torch.cuda.synchronize()
+            if dist:
+                dist.barrier()
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(steps):
+                fn()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1)
+            if dist:
+                t = torch.tensor([ms], device=f"cuda:{local}")
+                dist.all_reduce(t, op=dist.ReduceOp.MAX)
+                dist.barrier()
+                ms = float(t.item())
+            return ms / steps
+
+        def dev_step():
+            fp.dock_device(d_rot.data_ptr(), 0, nrot, T_POSES, d_pose.data_ptr())
+
+        # batched, device-resident inputs
+        fp.set_batch(batch)
+        with Clocks(local) as clk:
+            ms_batched = timed(dev_step, args.steps, args.warmup)
+        # plain form (one rotation per pipeline)
+        fp.set_batch(1)
+        ms_plain = timed(dev_step, max(1, args.steps // 2), 1)
+        # e2e through the C ABI with host buffers
+        fp.set_batch(batch)
+        host_rot = np.ascontiguousarray(mats)
+
+        def e2e_step():
+            fp.receptor_fft(rr, ri)
+            fp.ligand_data_transfer_gpu(xyz, rad, q, job.lig_core)
+            fp.cuda_fft(host_rot, t=T_POSES)
+
+        for _ in range(args.warmup):
+            e2e_step()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            e2e_step()
+        torch.cuda.synchronize()
+        ms_e2e = 1000.0 * (time.perf_counter() - t0) / args.steps
+        if dist:
+            t = torch.tensor([ms_e2e], device=f"cuda:{local}")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms_e2e = float(t.item())
+        # per-stage profile of the batched form (events on the launch stream)
+        stage_ms, launches_prof = fp.dock_profile(d_rot.data_ptr(), 0, nrot, T_POSES, d_pose.data_ptr())
+        fp.fft_memory_free()
+
+    if rank != 0:
+        if dist:
+            dist.destroy_process_group()
+        return
+
+    N3 = N_FFT ** 3
+    nb_launches = -(-nrot // batch)
+    # algorithmic bytes per rotation per stage (complex64 = 8 B)
+    stage_bytes = {
+        "plane_fwd": 8 * N3 // 2,            # write the ng non-zero spectrum planes
+        "xline": 8 * N3 // 2 + 8 * N3,       # read them, write the product after the inverse x pass
+        "plane_inv": 8 * N3,                 # read the x-inverted spectrum once
+        "merge": 0,
+    }
+    names = ["plane_fwd", "xline", "plane_inv", "merge"]
+    dom = max(range(4), key=lambda k: stage_ms[k])
+    dom_bytes_launch = stage_bytes[names[dom]] * batch + (8 * N3 if names[dom] == "xline" else 0)
+    dom_ms_launch = stage_ms[dom] / nb_launches
+    peak, peak_kind = _peaks()
+    achieved = dom_bytes_launch / (dom_ms_launch * 1e-3) / 1e9
+    traffic = None
+    tfile = ROOT / "profiles" / "traffic_per_rotation.json"
+    if tfile.exists():
+        tr = json.loads(tfile.read_text()).get(names[dom])
+        if tr:
+            traffic = tr * batch
+    value = world * nrot / (ms_batched * 1e-3)
+    plain = world * nrot / (ms_plain * 1e-3)
+    e2e = world * nrot / (ms_e2e * 1e-3)
+    model_bytes = 52 * N3
+    line = {
+        "metric": METRIC, "value": value, "unit": "rotations/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_batched, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"docking, {N_REC}/{N_LIG}-residue synthetic pair ({job.na_rec}/{job.na_lig} atoms), "
+                               f"N={N_FFT}, {ROT_SET} rotations, t={T_POSES}",
+                   "fft": N_FFT, "rotations": ROT_SET, "t": T_POSES, "rotations_per_launch": batch,
+                   "l2": "working set per step >> L2 (54,000 rotations x ~25 MB of intermediates)",
+                   "parallelism": f"replicas x{world}"},
+        "plain": {"value": plain, "ms_per_step": ms_plain, "unit": "rotations/s"},
+        "batched_over_plain": value / plain,
+        "e2e": {"value": e2e, "unit": "rotations/s", "ms_per_step": ms_e2e,
+                "h2d_bytes_per_step": int(rr.nbytes + ri.nbytes + mats.nbytes + xyz.nbytes + rad.nbytes + q.nbytes),
+                "d2h_bytes_per_step": int(nrot * T_POSES * 20)},
+        "roofline": {"bound": "hbm", "kernel": names[dom], "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
+                     "stage_ms": {n: float(stage_ms[k]) for k, n in enumerate(names)}},
+        "pipeline_model": {"bytes_per_rotation": model_bytes,
+                           "achieved_GBps": model_bytes * value / 1e9,
+                           "frac": model_bytes * value / 1e9 / peak},
+        "gpu_launches": int(args.steps * 4 * nb_launches),
+        "clocks": clk.summary(),
+    }
+    if not args.no_cpu_baseline:
+        try:
+            from oracle import ref
+            if ref.available():
+                with tempfile.TemporaryDirectory() as tmp:
+                    rp2, lp2 = make_inputs(tmp)
+                    v, cores, secs = cpu_reference(rp2, lp2)
+                line["cpu_baseline"] = {"value": v, "unit": "rotations/s", "cores": cores, "kind": "reference",
+                                        "sample": f"{REF_SAMPLE_ROT} rotations of the same job ({secs:.1f} s)"}
+        except Exception as e:  # the baseline is reported, never required
+            line["cpu_baseline"] = {"error": str(e)[:200]}
+    print(json.dumps(line))
+    if dist:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

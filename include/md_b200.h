@@ -1,0 +1,146 @@
+/*
+ * megadock-b200: C ABI of the B200-native per-rotation FFT docking path.
+ *
+ * The reference (akiyamalab/MEGADOCK) has no plugin API: its seam is the C++
+ * class FFTProcess (src/fft_process.h:168-195), called by Docking
+ * (src/docking.cpp).  Each entry point below states which FFTProcess /
+ * Docking / Control member it replaces.  Conventions:
+ *   - every function returns an int status, MD_OK (0) on success; nothing
+ *     calls exit() (the reference calls exit(1) on every error);
+ *   - md_last_error(ctx) (or md_job_error(job)) describes the last failure;
+ *   - host buffers are caller-owned; device buffers are owned by the context;
+ *   - one context per device, not shared between threads without a lock;
+ *   - all work is stream-ordered on the context's stream (md_set_stream).
+ */
+#ifndef MD_B200_H
+#define MD_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+    MD_OK = 0,
+    MD_ERR_ARG = 1,     /* bad argument (size, pointer, flag) */
+    MD_ERR_CUDA = 2,    /* CUDA runtime failure */
+    MD_ERR_STATE = 3,   /* call out of order (e.g. dock before receptor) */
+    MD_ERR_SIZE = 4,    /* FFT size / atom count beyond what is built */
+    MD_ERR_IO = 5,      /* file read/write failure */
+    MD_ERR_USAGE = 6    /* command-line usage error */
+};
+
+typedef struct md_ctx md_ctx;
+typedef struct md_job md_job;
+
+/* One docking pose.  Mirrors SortScore {float score; int index[4]}
+ * (src/fft_process.h:40-43): rot = index[0] (rotation number),
+ * i/j/k = index[1..3] (translation cell of the FFT grid). */
+typedef struct md_pose {
+    float score;
+    int rot, i, j, k;
+} md_pose;
+
+/* ------------------------------------------------------------ device context */
+
+/* Replaces the per-GPU set-up of FFTProcess::alloc_fft (src/fft_process.cpp:79-209)
+ * and main()'s device selection (src/main.cpp:75-110). */
+int md_ctx_create(int device, md_ctx **out);
+void md_ctx_destroy(md_ctx *ctx);               /* FFTProcess::fft_memory_free (:814-875) */
+const char *md_last_error(const md_ctx *ctx);
+/* Run all work on this cudaStream_t (NULL = the context's own stream). */
+int md_set_stream(md_ctx *ctx, void *cuda_stream);
+/* 1 when FFT edge nf1 has a built kernel set, else 0. */
+int md_fft_size_supported(int nf1);
+
+/* FFTProcess::alloc_array(num_fft) (src/fft_process.cpp:29-76) plus the grid
+ * centre coordinates of Docking::rec_init (src/docking.cpp:139-142).
+ * nf1 = 2 * ng1; grid_coord has ng1 entries. */
+int md_set_grid(md_ctx *ctx, int nf1, float grid_width, const float *grid_coord);
+
+/* FFTProcess::receptor_fft(grid_r, grid_i) (src/fft_process.cpp:212-303):
+ * embed the ng1^3 receptor grids at offset ng1/2 and take the forward 3D FFT
+ * on the device; the spectrum stays resident. */
+int md_receptor_fft(md_ctx *ctx, const float *grid_r, const float *grid_i);
+/* Copy the resident receptor spectrum (nf1^3 each, [x][y][z] order) back. */
+int md_receptor_spectrum(md_ctx *ctx, float *re, float *im);
+
+/* FFTProcess::ligand_data_transfer_gpu(grid_coord) (src/fft_process.cpp:769-807):
+ * centred atom coordinates (3*na), CHARMM radii and charges, and the ligand core
+ * value (-b, Ligand::rpscace's delta).  Core/surface radii are R*R*1.5 and
+ * R*R*1.0 as in Ligand::precalc (src/ligand.cpp:241-260). */
+int md_ligand_data(md_ctx *ctx, int na, const float *xyz_centred, const float *radius, const float *charge,
+                   float lig_core);
+
+/* Rotations per launch for md_dock (1 = the plain per-rotation pipeline;
+ * > 1 = the batched form, launched as one captured CUDA graph). */
+int md_set_batch(md_ctx *ctx, int rotations_per_launch);
+
+/* FFTProcess::cuda_fft (src/fft_process.cpp:502-656) over rotations
+ * [first_rot, first_rot + n_rot): rotate, voxelize, FFT, conj(R^) product,
+ * inverse FFT, top-t.  rotmat holds 9 floats per rotation (row-major, from
+ * md_rotation_matrix).  out receives n_rot * t poses, rotation-major, each
+ * rotation's poses best first (the _Top layout, src/fft_process.cpp:640-643).
+ * Host buffers; copies are included. */
+int md_dock(md_ctx *ctx, const float *rotmat, int first_rot, int n_rot, int t, md_pose *out);
+/* Same with device-resident rotation matrices and device output buffer. */
+int md_dock_device(md_ctx *ctx, const float *d_rotmat, int first_rot, int n_rot, int t, md_pose *d_out);
+
+/* Per-stage device time of md_dock_device's launches (no graph): stage_ms[4]
+ * receives the summed CUDA-event time of the rotate+voxelize+forward-plane
+ * kernel, the x-line product kernel, the inverse-plane top-t kernel and the
+ * merge kernel; *launches the number of kernel launches.  Replaces the
+ * reference's gettimeofday buckets (src/cpu_time.h:35-61). */
+int md_dock_profile(md_ctx *ctx, const float *d_rotmat, int first_rot, int n_rot, int t, md_pose *d_out,
+                    float *stage_ms, int *launches);
+
+/* Ligand::rpscace + Ligand::electro (src/ligand.cpp:20-239) of one rotation,
+ * computed by the device voxelizer; grid_r/grid_i receive ng1^3 floats. */
+int md_ligand_voxels(md_ctx *ctx, const float *rotmat9, float *grid_r, float *grid_i);
+
+/* ------------------------------------------------------------ host helpers */
+
+/* Rotation matrix of Docking::ligand_rotationz (src/docking.cpp:368-396) for
+ * ZXZ Euler angles theta[3]; m is row-major. */
+int md_rotation_matrix(const float *theta, float *m);
+
+/* FFTProcess::sort_index (src/fft_process.cpp:469-479): order poses by score,
+ * best first, for the first nout records (ties keep input order). */
+int md_sort_poses(md_pose *poses, int n, int nout);
+
+/* ------------------------------------------------------------ job (CLI) level */
+
+/* Parameter::initialize + Control::initialize (src/parameter.cpp:21-236,
+ * src/control.cpp:18-88): parse a MEGADOCK command line (argv[0] ignored),
+ * read the PDB files and tables, size the grid, build the receptor grids. */
+int md_job_create(int argc, const char **argv, md_job **out);
+const char *md_job_error(const md_job *job);
+/* Progress and warning text collected while the job was set up. */
+const char *md_job_log(const md_job *job);
+void md_job_destroy(md_job *job);
+/* Control::execute (src/control.cpp:468-529): dock every rotation on ctx and
+ * write the .out file.  ctx may be NULL (a context on device 0 is made). */
+int md_job_run(md_job *job, md_ctx *ctx);
+
+/* Job properties (valid after md_job_create). */
+int md_job_dims(const md_job *job, int *ng1, int *nf1, int *na_rec, int *na_lig, int *n_rot, int *t,
+                int *n_out);
+float md_job_grid_width(const md_job *job);
+const char *md_job_out_file(const md_job *job);
+int md_job_grid_coord(const md_job *job, float *out);                 /* ng1 */
+int md_job_receptor_grids(const md_job *job, float *grid_r, float *grid_i); /* ng1^3 */
+int md_job_ligand_atoms(const md_job *job, float *xyz_centred, float *radius, float *charge);
+int md_job_receptor_atoms(const md_job *job, float *xyz, float *radius, float *charge, float *ace);
+int md_job_centers(const md_job *job, float *rec_center, float *lig_center);
+int md_job_rotation_angles(const md_job *job, float *theta);         /* 3 * n_rot */
+float md_job_lig_core(const md_job *job);
+/* Poses of the last md_job_run (n_rot * t, rotation-major) and the merged top. */
+int md_job_poses(const md_job *job, md_pose *out);
+int md_job_top(const md_job *job, md_pose *out);                      /* n_out */
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,252 @@
+// Device FFT building blocks for the docking pipeline (sm_100a, FP32 complex).
+//
+// Every line transform is a two-level ("four-step") Cooley-Tukey split
+// N = R1 * R2 done by a group of threads over a shared-memory line:
+//   phase 1: item t in [0,R2) loads x[t + R2*m] (m < R1), does an R1-point DFT
+//            in registers, multiplies by W_N^(t*k1) and stores back to the same
+//            R1 positions (k1*R2 + t): it reads and writes one position set, so
+//            phase 1 needs no barrier between items;
+//   phase 2: item u in [0,R1) loads y[u*R2 + n2] (n2 < R2), does an R2-point
+//            DFT and yields X[u + R1*k2] in registers for the caller to store.
+// Lanes of a warp always index different lines and warps index the butterfly
+// item, so the inter-phase twiddle index t*k1 is warp-uniform (broadcast load).
+//
+// Zero padding: docking grids carry data only in the middle half of each axis
+// ([N/4, 3N/4)).  With R1 % 4 == 0 the pruned phase 1 loads exactly
+// m in [R1/4, 3R1/4) for every t and skips the other (zero) inputs.
+//
+// The small DFTs are generated at compile time: prime radices 2, 3, 5, 7, 11
+// are direct DFTs (radix 4 is a butterfly); composite radices recurse through
+// the same four-step split with constant twiddles folded by the compiler.
+// Trigonometric constants come from a constexpr Taylor series in double
+// (reduced to |x| <= pi), rounded once to float.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <type_traits>
+#include <utility>
+
+namespace mdb {
+
+// ------------------------------------------------------------------ constexpr trig
+namespace ct {
+constexpr double kPi = 3.14159265358979323846264338327950288;
+__host__ __device__ constexpr double sin_series(double x) {
+    double term = x, sum = x;
+    for (int n = 1; n < 24; ++n) {
+        term *= -x * x / ((2.0 * n) * (2.0 * n + 1.0));
+        sum += term;
+    }
+    return sum;
+}
+__host__ __device__ constexpr double cos_series(double x) {
+    double term = 1.0, sum = 1.0;
+    for (int n = 1; n < 24; ++n) {
+        term *= -x * x / ((2.0 * n - 1.0) * (2.0 * n));
+        sum += term;
+    }
+    return sum;
+}
+// angle 2*pi*k/n reduced to (-pi, pi]
+__host__ __device__ constexpr double red_angle(long k, long n) {
+    long m = ((k % n) + n) % n;
+    if (2 * m > n) m -= n;
+    return 2.0 * kPi * (double)m / (double)n;
+}
+__host__ __device__ constexpr float cos2pi(long k, long n) { return (float)cos_series(red_angle(k, n)); }
+__host__ __device__ constexpr float sin2pi(long k, long n) { return (float)sin_series(red_angle(k, n)); }
+
+__host__ __device__ constexpr int first_factor(int r) {
+    if (r % 4 == 0 && r != 4) return 4;
+    for (int p = 2; p * p <= r; ++p)
+        if (r % p == 0) return p;
+    return r;
+}
+}  // namespace ct
+
+// ------------------------------------------------------------------ complex helpers
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+    return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+// conj(a) * b
+__device__ __forceinline__ float2 cmulconj(float2 a, float2 b) {
+    return make_float2(a.x * b.x + a.y * b.y, a.x * b.y - a.y * b.x);
+}
+__device__ __forceinline__ float2 conjf2(float2 a) { return make_float2(a.x, -a.y); }
+
+template <int I, int N, class F>
+__device__ __forceinline__ void static_for(F &&f) {
+    if constexpr (I < N) {
+        f(std::integral_constant<int, I>{});
+        static_for<I + 1, N>(f);
+    }
+}
+
+// ------------------------------------------------------------------ small DFTs
+// In-place R-point DFT of v[0..R) with exponent sign S (-1 forward, +1 inverse):
+//   v[k] <- sum_n v[n] * exp(S * 2*pi*i*n*k/R)
+template <int R, int S, int F = ct::first_factor(R)>
+struct Dft;
+
+template <int S>
+struct Dft<1, S, 1> {
+    __device__ __forceinline__ static void run(float2 *) {}
+};
+
+template <int S>
+struct Dft<2, S, 2> {
+    __device__ __forceinline__ static void run(float2 *v) {
+        const float2 a = v[0], b = v[1];
+        v[0] = cadd(a, b);
+        v[1] = csub(a, b);
+    }
+};
+
+template <int S>
+struct Dft<4, S, 2> {
+    __device__ __forceinline__ static void run(float2 *v) {
+        const float2 t0 = cadd(v[0], v[2]), t1 = csub(v[0], v[2]);
+        const float2 t2 = cadd(v[1], v[3]), d = csub(v[1], v[3]);
+        // d * (S * i)
+        const float2 t3 = (S < 0) ? make_float2(d.y, -d.x) : make_float2(-d.y, d.x);
+        v[0] = cadd(t0, t2);
+        v[2] = csub(t0, t2);
+        v[1] = cadd(t1, t3);
+        v[3] = csub(t1, t3);
+    }
+};
+
+// Prime radix: direct DFT with symmetric pairing of n and R-n.
+template <int R, int S>
+struct Dft<R, S, R> {
+    static_assert(R % 2 == 1 && R >= 3, "odd prime radix");
+    __device__ __forceinline__ static void run(float2 *v) {
+        constexpr int H = (R - 1) / 2;
+        float2 sp[H], sm[H];
+        static_for<1, H + 1>([&](auto n_) {
+            constexpr int n = decltype(n_)::value;
+            sp[n - 1] = cadd(v[n], v[R - n]);
+            sm[n - 1] = csub(v[n], v[R - n]);
+        });
+        float2 out[R];
+        float2 dc = v[0];
+        static_for<0, H>([&](auto n) { dc = cadd(dc, sp[n]); });
+        out[0] = dc;
+        static_for<1, H + 1>([&](auto k_) {
+            constexpr int k = decltype(k_)::value;
+            float2 re = v[0];   // real-cosine part accumulation
+            float2 im = make_float2(0.f, 0.f);
+            static_for<1, H + 1>([&](auto n_) {
+                constexpr int n = decltype(n_)::value;
+                constexpr float c = ct::cos2pi((long)n * k, R);
+                constexpr float s = (float)S * ct::sin2pi((long)n * k, R);
+                re.x += c * sp[n - 1].x;
+                re.y += c * sp[n - 1].y;
+                // i * s * sm
+                im.x += -s * sm[n - 1].y;
+                im.y += s * sm[n - 1].x;
+            });
+            out[k] = cadd(re, im);
+            out[R - k] = csub(re, im);
+        });
+        static_for<0, R>([&](auto k) { v[k] = out[k]; });
+    }
+};
+
+// Composite radix: R = A * B, input n = B*n1 + n2, output k = k1 + A*k2.
+template <int R, int S, int A>
+struct Dft {
+    static constexpr int B = R / A;
+    __device__ __forceinline__ static void run(float2 *v) {
+        float2 tmp[R];
+        static_for<0, B>([&](auto n2_) {
+            constexpr int n2 = decltype(n2_)::value;
+            float2 a[A];
+            static_for<0, A>([&](auto n1_) {
+                constexpr int n1 = decltype(n1_)::value;
+                a[n1] = v[B * n1 + n2];
+            });
+            Dft<A, S>::run(a);
+            static_for<0, A>([&](auto k1_) {
+                constexpr int k1 = decltype(k1_)::value;
+                constexpr long e = (long)n2 * k1;
+                if constexpr (e % R == 0) {
+                    tmp[k1 * B + n2] = a[k1];
+                } else {
+                    constexpr float c = ct::cos2pi(e, R);
+                    constexpr float s = (float)S * ct::sin2pi(e, R);
+                    tmp[k1 * B + n2] = make_float2(a[k1].x * c - a[k1].y * s, a[k1].x * s + a[k1].y * c);
+                }
+            });
+        });
+        static_for<0, A>([&](auto k1_) {
+            constexpr int k1 = decltype(k1_)::value;
+            float2 b[B];
+            static_for<0, B>([&](auto n2_) { b[decltype(n2_)::value] = tmp[k1 * B + decltype(n2_)::value]; });
+            Dft<B, S>::run(b);
+            static_for<0, B>([&](auto k2_) { v[k1 + A * decltype(k2_)::value] = b[decltype(k2_)::value]; });
+        });
+    }
+};
+
+// ------------------------------------------------------------------ line plans
+// Supported FFT edge lengths and their split N = R1 * R2 (R1 % 4 == 0).
+template <int N>
+struct Plan;
+#define MDB_PLAN(N_, R1_, R2_)                                  \
+    template <>                                                  \
+    struct Plan<N_> {                                            \
+        static constexpr int R1 = R1_;                           \
+        static constexpr int R2 = R2_;                           \
+        static_assert(R1_ * R2_ == N_ && R1_ % 4 == 0, "plan");  \
+    };
+MDB_PLAN(32, 4, 8)
+MDB_PLAN(48, 4, 12)
+MDB_PLAN(64, 8, 8)
+MDB_PLAN(80, 8, 10)
+MDB_PLAN(96, 8, 12)
+MDB_PLAN(112, 8, 14)
+MDB_PLAN(120, 8, 15)
+MDB_PLAN(128, 8, 16)
+MDB_PLAN(144, 12, 12)
+MDB_PLAN(160, 16, 10)
+#undef MDB_PLAN
+
+// Phase 1 of one item on a line at `b` with element stride `es`.
+// tw: W_N^j = exp(-2*pi*i*j/N), j < N (forward table); S selects the sign.
+template <int N, int S, bool PRUNE>
+__device__ __forceinline__ void fft_phase1(float2 *b, int es, int t, const float2 *__restrict__ tw) {
+    constexpr int R1 = Plan<N>::R1, R2 = Plan<N>::R2;
+    float2 v[R1];
+    static_for<0, R1>([&](auto m_) {
+        constexpr int m = decltype(m_)::value;
+        if constexpr (PRUNE && (m < R1 / 4 || m >= 3 * R1 / 4)) {
+            v[m] = make_float2(0.f, 0.f);
+        } else {
+            v[m] = b[(t + R2 * m) * es];
+        }
+    });
+    Dft<R1, S>::run(v);
+    static_for<0, R1>([&](auto k1_) {
+        constexpr int k1 = decltype(k1_)::value;
+        float2 x = v[k1];
+        if constexpr (k1 != 0) {
+            float2 w = __ldg(&tw[t * k1]);
+            if (S > 0) w.y = -w.y;
+            x = cmul(x, w);
+        }
+        b[(k1 * R2 + t) * es] = x;
+    });
+}
+
+// Phase 2 load + DFT of item u; result out[k2] belongs at element u + R1*k2.
+template <int N, int S>
+__device__ __forceinline__ void fft_phase2(const float2 *b, int es, int u, float2 (&out)[Plan<N>::R2]) {
+    constexpr int R2 = Plan<N>::R2;
+    static_for<0, R2>([&](auto n2_) { out[decltype(n2_)::value] = b[(u * R2 + decltype(n2_)::value) * es]; });
+    Dft<R2, S>::run(out);
+}
+
+}  // namespace mdb

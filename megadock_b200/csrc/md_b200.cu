@@ -1,0 +1,546 @@
+// Device context and the device half of the C ABI (include/md_b200.h).
+//
+// Replaces FFTProcess's GPU members (src/fft_process.cpp:79-209 allocation,
+// :212-303 receptor FFT, :502-656 per-rotation pipeline, :660-807 ligand
+// voxelization and upload).  Differences by design:
+//   - one context per device, explicit stream, no cudaDeviceSynchronize inside
+//     the pipeline; a call returns after its own copies complete;
+//   - no cuFFT: every transform is the project's fused FFT (dock_kernels.cuh);
+//   - errors are returned as status codes with a message, never exit().
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "../../include/md_b200.h"
+#include "dock_kernels.cuh"
+
+using namespace mdb;
+
+struct md_ctx {
+    int device = 0;
+    cudaStream_t own = nullptr;
+    cudaStream_t stream = nullptr;
+    std::string err;
+    // grid
+    int N = 0, ng = 0;
+    float gw = 0.f;
+    float *d_gc = nullptr;
+    float2 *d_tw = nullptr;
+    // receptor spectrum [kx][ky][kz]
+    float2 *d_Rh = nullptr;
+    bool have_receptor = false;
+    // ligand
+    int na = 0;
+    float delta = 1.0f;
+    float4 *d_atom = nullptr;
+    float2 *d_rad2 = nullptr;
+    bool have_ligand = false;
+    // per-launch work buffers, sized for `cap` rotations
+    int batch = 1;
+    int cap = 0;
+    int cap_t = 0;
+    float2 *d_A = nullptr;   // [cap][ng][N][N]
+    float2 *d_G = nullptr;   // [cap][N][N][N]
+    Cand *d_cand = nullptr;  // [cap][N][t]
+    // staging for host-buffer calls
+    float *d_rot = nullptr;
+    size_t rot_cap = 0;
+    DevPose *d_pose = nullptr;
+    size_t pose_cap = 0;
+    // captured graphs of the batched form: (first_rot, n_rot, t, batch, rot ptr, pose ptr)
+    std::map<std::tuple<int, int, int, int, const float *, DevPose *>, cudaGraphExec_t> graphs;
+};
+
+static_assert(sizeof(md_pose) == sizeof(DevPose), "pose layout");
+
+#define MD_CUDA(call)                                                                          \
+    do {                                                                                       \
+        cudaError_t e_ = (call);                                                               \
+        if (e_ != cudaSuccess) {                                                               \
+            ctx->err = std::string(#call) + ": " + cudaGetErrorString(e_);                     \
+            return MD_ERR_CUDA;                                                                \
+        }                                                                                      \
+    } while (0)
+
+namespace {
+
+// ------------------------------------------------------------------ per-size dispatch
+template <int N>
+struct Sized {
+    static constexpr int NG = N / 2;
+    static size_t smem_plane() { return (size_t)N * (N + 1) * sizeof(float2); }
+    static size_t smem_fwd() { return smem_plane() + (kMaxLigAtoms / 32) * sizeof(uint32_t); }
+
+    static cudaError_t set_attrs() {
+        static bool done = false;
+        if (done) return cudaSuccess;
+        cudaError_t e;
+        if ((e = cudaFuncSetAttribute(k_plane_fwd<N, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)smem_fwd())) != cudaSuccess)
+            return e;
+        if ((e = cudaFuncSetAttribute(k_plane_fwd<N, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)smem_fwd())) != cudaSuccess)
+            return e;
+        if ((e = cudaFuncSetAttribute(k_plane_fwd<N, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)smem_fwd())) != cudaSuccess)
+            return e;
+        if ((e = cudaFuncSetAttribute(k_plane_inv<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)smem_plane())) != cudaSuccess)
+            return e;
+        done = true;
+        return cudaSuccess;
+    }
+
+    static void receptor(md_ctx *c, const float *d_r, const float *d_i) {
+        GridView G{c->ng, c->gw, 0.f, c->d_gc, c->d_tw};
+        LigandView L{0, nullptr, nullptr, 1.f};
+        k_plane_fwd<N, 1><<<dim3(NG, 1), kNT, smem_fwd(), c->stream>>>(L, G, nullptr, d_r, d_i, c->d_A, nullptr,
+                                                                        nullptr);
+        k_xline<N, 1><<<dim3(N * (N / kLT), 1), kNT, 0, c->stream>>>(G, c->d_A, nullptr, c->d_Rh);
+    }
+
+    static void voxels(md_ctx *c, const float *d_rot9, float *d_vr, float *d_vi) {
+        GridView G{c->ng, c->gw, (float)(c->ng * c->gw) / 2, c->d_gc, c->d_tw};
+        LigandView L{c->na, c->d_atom, c->d_rad2, c->delta};
+        k_plane_fwd<N, 2><<<dim3(NG, 1), kNT, smem_fwd(), c->stream>>>(L, G, d_rot9, nullptr, nullptr, nullptr, d_vr,
+                                                                        d_vi);
+    }
+
+    // One launch group: nb rotations whose matrices start at d_rot9.  With
+    // `ev` set, an event is recorded after each of the four kernels.
+    static void dock(md_ctx *c, const float *d_rot9, int nb, int rot0, int t, DevPose *d_pose,
+                     cudaEvent_t *ev = nullptr) {
+        GridView G{c->ng, c->gw, (float)(c->ng * c->gw) / 2, c->d_gc, c->d_tw};
+        LigandView L{c->na, c->d_atom, c->d_rad2, c->delta};
+        const float nf3f = (float)((long long)N * N * N);
+        k_plane_fwd<N, 0><<<dim3(NG, nb), kNT, smem_fwd(), c->stream>>>(L, G, d_rot9, nullptr, nullptr, c->d_A,
+                                                                         nullptr, nullptr);
+        if (ev) cudaEventRecord(ev[1], c->stream);
+        k_xline<N, 0><<<dim3(N * (N / kLT), nb), kNT, 0, c->stream>>>(G, c->d_A, c->d_Rh, c->d_G);
+        if (ev) cudaEventRecord(ev[2], c->stream);
+        k_plane_inv<N><<<dim3(N, nb), kNT, smem_plane(), c->stream>>>(G, c->d_G, t, nf3f, c->d_cand);
+        if (ev) cudaEventRecord(ev[3], c->stream);
+        k_merge<<<nb, 256, 0, c->stream>>>(c->d_cand, N, t, N, nf3f, rot0, d_pose);
+        if (ev) cudaEventRecord(ev[4], c->stream);
+    }
+};
+
+#define MDB_SIZES(X) X(32) X(48) X(64) X(80) X(96) X(112) X(120) X(128) X(144) X(160)
+
+bool size_supported(int N) {
+    switch (N) {
+#define X(n) case n:
+        MDB_SIZES(X)
+#undef X
+        return true;
+    default:
+        return false;
+    }
+}
+
+cudaError_t set_attrs(int N) {
+    switch (N) {
+#define X(n) \
+    case n: return Sized<n>::set_attrs();
+        MDB_SIZES(X)
+#undef X
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+void launch_receptor(md_ctx *c, const float *r, const float *i) {
+    switch (c->N) {
+#define X(n) \
+    case n: Sized<n>::receptor(c, r, i); break;
+        MDB_SIZES(X)
+#undef X
+    }
+}
+
+void launch_voxels(md_ctx *c, const float *rot, float *vr, float *vi) {
+    switch (c->N) {
+#define X(n) \
+    case n: Sized<n>::voxels(c, rot, vr, vi); break;
+        MDB_SIZES(X)
+#undef X
+    }
+}
+
+void launch_dock(md_ctx *c, const float *rot, int nb, int rot0, int t, DevPose *pose, cudaEvent_t *ev = nullptr) {
+    switch (c->N) {
+#define X(n) \
+    case n: Sized<n>::dock(c, rot, nb, rot0, t, pose, ev); break;
+        MDB_SIZES(X)
+#undef X
+    }
+}
+
+void free_graphs(md_ctx *c) {
+    for (auto &kv : c->graphs) cudaGraphExecDestroy(kv.second);
+    c->graphs.clear();
+}
+
+int ensure_work(md_ctx *ctx, int cap, int t) {
+    if (cap <= ctx->cap && t <= ctx->cap_t) return MD_OK;
+    free_graphs(ctx);
+    cudaFree(ctx->d_A);
+    cudaFree(ctx->d_G);
+    cudaFree(ctx->d_cand);
+    ctx->d_A = nullptr;
+    ctx->d_G = nullptr;
+    ctx->d_cand = nullptr;
+    ctx->cap = ctx->cap_t = 0;
+    const size_t N = ctx->N, NG = ctx->ng;
+    cap = std::max(cap, 1);
+    t = std::max(t, 1);
+    MD_CUDA(cudaMalloc(&ctx->d_A, sizeof(float2) * cap * NG * N * N));
+    MD_CUDA(cudaMalloc(&ctx->d_G, sizeof(float2) * cap * N * N * N));
+    MD_CUDA(cudaMalloc(&ctx->d_cand, sizeof(Cand) * cap * N * t));
+    ctx->cap = cap;
+    ctx->cap_t = t;
+    return MD_OK;
+}
+
+int check_ready(md_ctx *ctx) {
+    if (!ctx->N) {
+        ctx->err = "md_set_grid has not been called";
+        return MD_ERR_STATE;
+    }
+    if (!ctx->have_receptor) {
+        ctx->err = "md_receptor_fft has not been called";
+        return MD_ERR_STATE;
+    }
+    if (!ctx->have_ligand) {
+        ctx->err = "md_ligand_data has not been called";
+        return MD_ERR_STATE;
+    }
+    return MD_OK;
+}
+
+// The rotation loop of one md_dock call on device buffers.
+int run_dock(md_ctx *ctx, const float *d_rot, int first_rot, int n_rot, int t, DevPose *d_pose) {
+    const int B = std::max(1, std::min(ctx->batch, n_rot));
+    int rc = ensure_work(ctx, B, t);
+    if (rc) return rc;
+    if (B == 1) {
+        // plain form: one rotation per fused pipeline, launched back to back
+        for (int r = 0; r < n_rot; ++r) launch_dock(ctx, d_rot + 9 * (size_t)r, 1, first_rot + r, t, d_pose + (size_t)r * t);
+        MD_CUDA(cudaGetLastError());
+        return MD_OK;
+    }
+    // batched form: the whole rotation loop as one captured CUDA graph
+    auto key = std::make_tuple(first_rot, n_rot, t, B, d_rot, d_pose);
+    auto it = ctx->graphs.find(key);
+    if (it == ctx->graphs.end()) {
+        cudaGraph_t g;
+        MD_CUDA(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+        for (int r = 0; r < n_rot; r += B) {
+            const int nb = std::min(B, n_rot - r);
+            launch_dock(ctx, d_rot + 9 * (size_t)r, nb, first_rot + r, t, d_pose + (size_t)r * t);
+        }
+        cudaError_t ce = cudaStreamEndCapture(ctx->stream, &g);
+        if (ce != cudaSuccess) {
+            ctx->err = std::string("graph capture: ") + cudaGetErrorString(ce);
+            return MD_ERR_CUDA;
+        }
+        cudaGraphExec_t ex;
+        ce = cudaGraphInstantiate(&ex, g, 0);
+        cudaGraphDestroy(g);
+        if (ce != cudaSuccess) {
+            ctx->err = std::string("graph instantiate: ") + cudaGetErrorString(ce);
+            return MD_ERR_CUDA;
+        }
+        it = ctx->graphs.emplace(key, ex).first;
+    }
+    MD_CUDA(cudaGraphLaunch(it->second, ctx->stream));
+    return MD_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int md_fft_size_supported(int nf1) { return size_supported(nf1) ? 1 : 0; }
+
+int md_ctx_create(int device, md_ctx **out) {
+    if (!out) return MD_ERR_ARG;
+    *out = nullptr;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) return MD_ERR_CUDA;
+    if (device < 0 || device >= n) return MD_ERR_ARG;
+    md_ctx *ctx = new md_ctx;
+    ctx->device = device;
+    if (cudaSetDevice(device) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&ctx->own, cudaStreamNonBlocking) != cudaSuccess) {
+        delete ctx;
+        return MD_ERR_CUDA;
+    }
+    ctx->stream = ctx->own;
+    *out = ctx;
+    return MD_OK;
+}
+
+void md_ctx_destroy(md_ctx *ctx) {
+    if (!ctx) return;
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    free_graphs(ctx);
+    cudaFree(ctx->d_gc);
+    cudaFree(ctx->d_tw);
+    cudaFree(ctx->d_Rh);
+    cudaFree(ctx->d_atom);
+    cudaFree(ctx->d_rad2);
+    cudaFree(ctx->d_A);
+    cudaFree(ctx->d_G);
+    cudaFree(ctx->d_cand);
+    cudaFree(ctx->d_rot);
+    cudaFree(ctx->d_pose);
+    if (ctx->own) cudaStreamDestroy(ctx->own);
+    delete ctx;
+}
+
+const char *md_last_error(const md_ctx *ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+int md_set_stream(md_ctx *ctx, void *stream) {
+    if (!ctx) return MD_ERR_ARG;
+    free_graphs(ctx);
+    ctx->stream = stream ? (cudaStream_t)stream : ctx->own;
+    return MD_OK;
+}
+
+int md_set_grid(md_ctx *ctx, int nf1, float grid_width, const float *grid_coord) {
+    if (!ctx || !grid_coord || !(grid_width > 0.f)) return MD_ERR_ARG;
+    if (!size_supported(nf1)) {
+        ctx->err = "FFT size " + std::to_string(nf1) + " has no built kernel set";
+        return MD_ERR_SIZE;
+    }
+    MD_CUDA(cudaSetDevice(ctx->device));
+    MD_CUDA(set_attrs(nf1));
+    if (ctx->N != nf1) {
+        free_graphs(ctx);
+        cudaFree(ctx->d_gc);
+        cudaFree(ctx->d_tw);
+        cudaFree(ctx->d_Rh);
+        cudaFree(ctx->d_A);
+        cudaFree(ctx->d_G);
+        cudaFree(ctx->d_cand);
+        ctx->d_gc = nullptr;
+        ctx->d_tw = nullptr;
+        ctx->d_Rh = nullptr;
+        ctx->d_A = ctx->d_G = nullptr;
+        ctx->d_cand = nullptr;
+        ctx->cap = ctx->cap_t = 0;
+        ctx->have_receptor = false;
+        const size_t N = nf1;
+        MD_CUDA(cudaMalloc(&ctx->d_gc, sizeof(float) * N / 2));
+        MD_CUDA(cudaMalloc(&ctx->d_tw, sizeof(float2) * N));
+        MD_CUDA(cudaMalloc(&ctx->d_Rh, sizeof(float2) * N * N * N));
+        std::vector<float2> tw(N);
+        for (size_t j = 0; j < N; ++j) {
+            const double a = -2.0 * M_PI * (double)j / (double)N;
+            tw[j] = make_float2((float)std::cos(a), (float)std::sin(a));
+        }
+        MD_CUDA(cudaMemcpyAsync(ctx->d_tw, tw.data(), sizeof(float2) * N, cudaMemcpyHostToDevice, ctx->stream));
+        MD_CUDA(cudaStreamSynchronize(ctx->stream));
+        ctx->N = nf1;
+        ctx->ng = nf1 / 2;
+    }
+    ctx->gw = grid_width;
+    MD_CUDA(cudaMemcpyAsync(ctx->d_gc, grid_coord, sizeof(float) * ctx->ng, cudaMemcpyHostToDevice, ctx->stream));
+    MD_CUDA(cudaStreamSynchronize(ctx->stream));
+    return MD_OK;
+}
+
+int md_receptor_fft(md_ctx *ctx, const float *grid_r, const float *grid_i) {
+    if (!ctx || !grid_r || !grid_i) return MD_ERR_ARG;
+    if (!ctx->N) {
+        ctx->err = "md_set_grid has not been called";
+        return MD_ERR_STATE;
+    }
+    MD_CUDA(cudaSetDevice(ctx->device));
+    int rc = ensure_work(ctx, std::max(1, ctx->batch), 1);
+    if (rc) return rc;
+    const size_t ng3 = (size_t)ctx->ng * ctx->ng * ctx->ng;
+    float *d_r = nullptr, *d_i = nullptr;
+    MD_CUDA(cudaMalloc(&d_r, sizeof(float) * ng3 * 2));
+    d_i = d_r + ng3;
+    MD_CUDA(cudaMemcpyAsync(d_r, grid_r, sizeof(float) * ng3, cudaMemcpyHostToDevice, ctx->stream));
+    MD_CUDA(cudaMemcpyAsync(d_i, grid_i, sizeof(float) * ng3, cudaMemcpyHostToDevice, ctx->stream));
+    launch_receptor(ctx, d_r, d_i);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    cudaFree(d_r);
+    if (e != cudaSuccess) {
+        ctx->err = std::string("receptor FFT: ") + cudaGetErrorString(e);
+        return MD_ERR_CUDA;
+    }
+    ctx->have_receptor = true;
+    return MD_OK;
+}
+
+int md_receptor_spectrum(md_ctx *ctx, float *re, float *im) {
+    if (!ctx || !re || !im) return MD_ERR_ARG;
+    if (!ctx->have_receptor) {
+        ctx->err = "no receptor spectrum";
+        return MD_ERR_STATE;
+    }
+    const size_t n3 = (size_t)ctx->N * ctx->N * ctx->N;
+    std::vector<float2> h(n3);
+    MD_CUDA(cudaMemcpyAsync(h.data(), ctx->d_Rh, sizeof(float2) * n3, cudaMemcpyDeviceToHost, ctx->stream));
+    MD_CUDA(cudaStreamSynchronize(ctx->stream));
+    for (size_t i = 0; i < n3; ++i) {
+        re[i] = h[i].x;
+        im[i] = h[i].y;
+    }
+    return MD_OK;
+}
+
+int md_ligand_data(md_ctx *ctx, int na, const float *xyz, const float *radius, const float *charge,
+                   float lig_core) {
+    if (!ctx || na <= 0 || !xyz || !radius || !charge) return MD_ERR_ARG;
+    if (na > kMaxLigAtoms) {
+        ctx->err = "ligand has " + std::to_string(na) + " atoms; at most " + std::to_string(kMaxLigAtoms) +
+                   " are supported";
+        return MD_ERR_SIZE;
+    }
+    if (lig_core == 0.0f || lig_core == -8888.0f) {
+        ctx->err = "ligand core value (-b) 0 or -8888 collides with the voxelizer's markers";
+        return MD_ERR_ARG;
+    }
+    MD_CUDA(cudaSetDevice(ctx->device));
+    std::vector<float4> atom(na);
+    std::vector<float2> rad(na);
+    for (int l = 0; l < na; ++l) {
+        atom[l] = make_float4(xyz[3 * l], xyz[3 * l + 1], xyz[3 * l + 2], charge[l]);
+        // Ligand::precalc (src/ligand.cpp:251-254): R*R*1.5 and R*R*1.0 in float
+        const float r = radius[l];
+        rad[l] = make_float2(r * r * 1.5f, r * r * 1.0f);
+    }
+    cudaFree(ctx->d_atom);
+    cudaFree(ctx->d_rad2);
+    ctx->d_atom = nullptr;
+    ctx->d_rad2 = nullptr;
+    MD_CUDA(cudaMalloc(&ctx->d_atom, sizeof(float4) * na));
+    MD_CUDA(cudaMalloc(&ctx->d_rad2, sizeof(float2) * na));
+    MD_CUDA(cudaMemcpyAsync(ctx->d_atom, atom.data(), sizeof(float4) * na, cudaMemcpyHostToDevice, ctx->stream));
+    MD_CUDA(cudaMemcpyAsync(ctx->d_rad2, rad.data(), sizeof(float2) * na, cudaMemcpyHostToDevice, ctx->stream));
+    MD_CUDA(cudaStreamSynchronize(ctx->stream));
+    ctx->na = na;
+    ctx->delta = lig_core;
+    ctx->have_ligand = true;
+    free_graphs(ctx);
+    return MD_OK;
+}
+
+int md_set_batch(md_ctx *ctx, int b) {
+    if (!ctx || b < 1) return MD_ERR_ARG;
+    ctx->batch = b;
+    return MD_OK;
+}
+
+int md_dock_device(md_ctx *ctx, const float *d_rot, int first_rot, int n_rot, int t, md_pose *d_out) {
+    if (!ctx || !d_rot || !d_out || n_rot < 0 || t < 1) return MD_ERR_ARG;
+    int rc = check_ready(ctx);
+    if (rc) return rc;
+    if (n_rot == 0) return MD_OK;
+    MD_CUDA(cudaSetDevice(ctx->device));
+    return run_dock(ctx, d_rot, first_rot, n_rot, t, reinterpret_cast<DevPose *>(d_out));
+}
+
+int md_dock(md_ctx *ctx, const float *rotmat, int first_rot, int n_rot, int t, md_pose *out) {
+    if (!ctx || !rotmat || !out || n_rot < 0 || t < 1) return MD_ERR_ARG;
+    int rc = check_ready(ctx);
+    if (rc) return rc;
+    if (n_rot == 0) return MD_OK;
+    MD_CUDA(cudaSetDevice(ctx->device));
+    if ((size_t)n_rot * 9 > ctx->rot_cap) {
+        free_graphs(ctx);
+        cudaFree(ctx->d_rot);
+        ctx->d_rot = nullptr;
+        ctx->rot_cap = 0;
+        MD_CUDA(cudaMalloc(&ctx->d_rot, sizeof(float) * 9 * n_rot));
+        ctx->rot_cap = (size_t)n_rot * 9;
+    }
+    if ((size_t)n_rot * t > ctx->pose_cap) {
+        free_graphs(ctx);
+        cudaFree(ctx->d_pose);
+        ctx->d_pose = nullptr;
+        ctx->pose_cap = 0;
+        MD_CUDA(cudaMalloc(&ctx->d_pose, sizeof(DevPose) * n_rot * t));
+        ctx->pose_cap = (size_t)n_rot * t;
+    }
+    MD_CUDA(cudaMemcpyAsync(ctx->d_rot, rotmat, sizeof(float) * 9 * n_rot, cudaMemcpyHostToDevice, ctx->stream));
+    rc = run_dock(ctx, ctx->d_rot, first_rot, n_rot, t, ctx->d_pose);
+    if (rc) return rc;
+    MD_CUDA(cudaMemcpyAsync(out, ctx->d_pose, sizeof(DevPose) * n_rot * t, cudaMemcpyDeviceToHost, ctx->stream));
+    MD_CUDA(cudaStreamSynchronize(ctx->stream));
+    return MD_OK;
+}
+
+int md_dock_profile(md_ctx *ctx, const float *d_rot, int first_rot, int n_rot, int t, md_pose *d_out,
+                    float *stage_ms, int *launches) {
+    if (!ctx || !d_rot || !d_out || !stage_ms || n_rot < 1 || t < 1) return MD_ERR_ARG;
+    int rc = check_ready(ctx);
+    if (rc) return rc;
+    MD_CUDA(cudaSetDevice(ctx->device));
+    const int B = std::max(1, std::min(ctx->batch, n_rot));
+    if ((rc = ensure_work(ctx, B, t))) return rc;
+    cudaEvent_t ev[5];
+    for (auto &e : ev) MD_CUDA(cudaEventCreate(&e));
+    double acc[4] = {0, 0, 0, 0};
+    int nl = 0;
+    for (int r = 0; r < n_rot; r += B) {
+        const int nb = std::min(B, n_rot - r);
+        MD_CUDA(cudaEventRecord(ev[0], ctx->stream));
+        launch_dock(ctx, d_rot + 9 * (size_t)r, nb, first_rot + r, t,
+                    reinterpret_cast<DevPose *>(d_out) + (size_t)r * t, ev);
+        nl += 4;
+        MD_CUDA(cudaEventSynchronize(ev[4]));
+        for (int k = 0; k < 4; ++k) {
+            float ms = 0.f;
+            MD_CUDA(cudaEventElapsedTime(&ms, ev[k], ev[k + 1]));
+            acc[k] += ms;
+        }
+    }
+    for (auto &e : ev) cudaEventDestroy(e);
+    for (int k = 0; k < 4; ++k) stage_ms[k] = (float)acc[k];
+    if (launches) *launches = nl;
+    MD_CUDA(cudaGetLastError());
+    return MD_OK;
+}
+
+int md_ligand_voxels(md_ctx *ctx, const float *rotmat9, float *grid_r, float *grid_i) {
+    if (!ctx || !rotmat9 || !grid_r || !grid_i) return MD_ERR_ARG;
+    if (!ctx->N || !ctx->have_ligand) {
+        ctx->err = "grid and ligand must be set first";
+        return MD_ERR_STATE;
+    }
+    MD_CUDA(cudaSetDevice(ctx->device));
+    const size_t ng3 = (size_t)ctx->ng * ctx->ng * ctx->ng;
+    float *d = nullptr;
+    MD_CUDA(cudaMalloc(&d, sizeof(float) * (ng3 * 2 + 9)));
+    float *d_vr = d, *d_vi = d + ng3, *d_rot = d + 2 * ng3;
+    cudaError_t e = cudaMemcpyAsync(d_rot, rotmat9, sizeof(float) * 9, cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess) {
+        launch_voxels(ctx, d_rot, d_vr, d_vi);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(grid_r, d_vr, sizeof(float) * ng3, cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(grid_i, d_vi, sizeof(float) * ng3, cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    cudaFree(d);
+    if (e != cudaSuccess) {
+        ctx->err = std::string("voxelization: ") + cudaGetErrorString(e);
+        return MD_ERR_CUDA;
+    }
+    return MD_OK;
+}
+
+}  // extern "C"

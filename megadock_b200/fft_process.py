@@ -1,0 +1,209 @@
+"""Python mirror of MEGADOCK's docking-path interface over the C ABI.
+
+``FFTProcess`` keeps the method names and argument meaning of the reference's
+class (src/fft_process.h:168-195) so callers and tests read like MEGADOCK's
+own driver (src/docking.cpp:194-346): alloc_array, receptor_fft,
+ligand_data_transfer_gpu, cuda_fft, sort_index, top_score, top_index,
+fft_memory_free.  Errors raise ``MdError`` instead of calling exit().
+
+``Job`` mirrors ``Control`` (src/control.cpp): a MEGADOCK command line parsed,
+sized and run end to end, writing the same .out file.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _native as N
+from ._native import MdError, POSE_DTYPE
+
+
+def _check(rc, ctx=None, what=""):
+    if rc:
+        msg = N.lib().md_last_error(ctx).decode() if ctx else what
+        raise MdError(rc, msg or what)
+
+
+class FFTProcess:
+    """Device context for one receptor-ligand pair on one GPU."""
+
+    def __init__(self, device: int = 0, stream: int | None = None):
+        h = C.c_void_p()
+        _check(N.lib().md_ctx_create(device, C.byref(h)), None, "md_ctx_create")
+        self._h = h
+        self.num_fft = 0
+        self._top = None
+        if stream is not None:
+            _check(N.lib().md_set_stream(self._h, C.c_void_p(stream)), self._h)
+
+    # -- FFTProcess::alloc_array(num_fft) + Docking::rec_init grid coordinates
+    def alloc_array(self, num_fft: int, grid_width: float, grid_coord: np.ndarray):
+        gc = np.ascontiguousarray(grid_coord, dtype=np.float32)
+        _check(N.lib().md_set_grid(self._h, int(num_fft), float(grid_width), N.fptr(gc)), self._h)
+        self.num_fft = int(num_fft)
+
+    # -- FFTProcess::receptor_fft(grid_r, grid_i)
+    def receptor_fft(self, grid_r: np.ndarray, grid_i: np.ndarray):
+        r = np.ascontiguousarray(grid_r, dtype=np.float32)
+        i = np.ascontiguousarray(grid_i, dtype=np.float32)
+        _check(N.lib().md_receptor_fft(self._h, N.fptr(r), N.fptr(i)), self._h)
+
+    def receptor_spectrum(self) -> np.ndarray:
+        n3 = self.num_fft ** 3
+        re = np.zeros(n3, np.float32)
+        im = np.zeros(n3, np.float32)
+        _check(N.lib().md_receptor_spectrum(self._h, N.fptr(re), N.fptr(im)), self._h)
+        return (re + 1j * im.astype(np.complex64)).reshape((self.num_fft,) * 3)
+
+    # -- FFTProcess::ligand_data_transfer_gpu(grid_coord)
+    def ligand_data_transfer_gpu(self, xyz_centred, radius, charge, lig_core: float = 1.0):
+        xyz = np.ascontiguousarray(xyz_centred, dtype=np.float32).reshape(-1)
+        rad = np.ascontiguousarray(radius, dtype=np.float32)
+        q = np.ascontiguousarray(charge, dtype=np.float32)
+        _check(N.lib().md_ligand_data(self._h, len(rad), N.fptr(xyz), N.fptr(rad), N.fptr(q), float(lig_core)),
+               self._h)
+
+    def set_batch(self, rotations_per_launch: int):
+        _check(N.lib().md_set_batch(self._h, int(rotations_per_launch)), self._h)
+
+    # -- FFTProcess::cuda_fft over a rotation range
+    def cuda_fft(self, rotmats: np.ndarray, t: int = 1, first_rot: int = 0) -> np.ndarray:
+        m = np.ascontiguousarray(rotmats, dtype=np.float32).reshape(-1, 9)
+        out = np.zeros(len(m) * t, POSE_DTYPE)
+        _check(N.lib().md_dock(self._h, N.fptr(m), int(first_rot), len(m), int(t), N.vptr(out)), self._h)
+        self._top = out
+        return out
+
+    def dock_device(self, d_rotmat: int, first_rot: int, n_rot: int, t: int, d_out: int):
+        _check(N.lib().md_dock_device(self._h, C.c_void_p(d_rotmat), first_rot, n_rot, t, C.c_void_p(d_out)),
+               self._h)
+
+    def dock_profile(self, d_rotmat: int, first_rot: int, n_rot: int, t: int, d_out: int):
+        """Per-stage device milliseconds (4 stages) and the launch count."""
+        ms = np.zeros(4, np.float32)
+        nl = C.c_int()
+        _check(N.lib().md_dock_profile(self._h, C.c_void_p(d_rotmat), first_rot, n_rot, t, C.c_void_p(d_out),
+                                       N.fptr(ms), C.byref(nl)), self._h)
+        return ms, nl.value
+
+    def ligand_voxels(self, rotmat9: np.ndarray):
+        m = np.ascontiguousarray(rotmat9, dtype=np.float32).reshape(9)
+        ng = self.num_fft // 2
+        r = np.zeros(ng ** 3, np.float32)
+        i = np.zeros(ng ** 3, np.float32)
+        _check(N.lib().md_ligand_voxels(self._h, N.fptr(m), N.fptr(r), N.fptr(i)), self._h)
+        return r.reshape((ng,) * 3), i.reshape((ng,) * 3)
+
+    # -- FFTProcess::sort_index / top_score / top_index
+    def sort_index(self, nout: int):
+        self._top = N.sort_poses(self._top, nout)
+
+    def top_score(self, j: int) -> float:
+        return float(self._top[j]["score"])
+
+    def top_index(self, j: int, k: int) -> int:
+        return int(self._top[j][("rot", "i", "j", "k")[k]])
+
+    # -- FFTProcess::fft_memory_free
+    def fft_memory_free(self):
+        if getattr(self, "_h", None):
+            N.lib().md_ctx_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.fft_memory_free()
+        except Exception:
+            pass
+
+
+class Job:
+    """A MEGADOCK command line (Control::initialize / Control::execute)."""
+
+    def __init__(self, args):
+        argv = ["megadock-b200"] + [str(a) for a in args]
+        arr = (C.c_char_p * len(argv))(*[a.encode() for a in argv])
+        h = C.c_void_p()
+        rc = N.lib().md_job_create(len(argv), arr, C.byref(h))
+        self._h = h
+        if rc:
+            msg = N.lib().md_job_error(h).decode()
+            self.close()
+            raise MdError(rc, msg)
+        dims = [C.c_int() for _ in range(7)]
+        N.lib().md_job_dims(self._h, *[C.byref(d) for d in dims])
+        self.ng1, self.nf1, self.na_rec, self.na_lig, self.n_rot, self.t, self.n_out = [d.value for d in dims]
+        self.grid_width = N.lib().md_job_grid_width(self._h)
+        self.lig_core = N.lib().md_job_lig_core(self._h)
+
+    @property
+    def log(self) -> str:
+        return N.lib().md_job_log(self._h).decode()
+
+    @property
+    def out_file(self) -> str:
+        return N.lib().md_job_out_file(self._h).decode()
+
+    def grid_coord(self):
+        a = np.zeros(self.ng1, np.float32)
+        N.lib().md_job_grid_coord(self._h, N.fptr(a))
+        return a
+
+    def receptor_grids(self):
+        n = self.ng1 ** 3
+        r = np.zeros(n, np.float32)
+        i = np.zeros(n, np.float32)
+        N.lib().md_job_receptor_grids(self._h, N.fptr(r), N.fptr(i))
+        return r.reshape((self.ng1,) * 3), i.reshape((self.ng1,) * 3)
+
+    def ligand_atoms(self):
+        xyz = np.zeros(3 * self.na_lig, np.float32)
+        rad = np.zeros(self.na_lig, np.float32)
+        q = np.zeros(self.na_lig, np.float32)
+        N.lib().md_job_ligand_atoms(self._h, N.fptr(xyz), N.fptr(rad), N.fptr(q))
+        return xyz.reshape(-1, 3), rad, q
+
+    def receptor_atoms(self):
+        n = self.na_rec
+        xyz, rad, q, ace = (np.zeros(3 * n, np.float32), np.zeros(n, np.float32), np.zeros(n, np.float32),
+                            np.zeros(n, np.float32))
+        N.lib().md_job_receptor_atoms(self._h, N.fptr(xyz), N.fptr(rad), N.fptr(q), N.fptr(ace))
+        return xyz.reshape(-1, 3), rad, q, ace
+
+    def centers(self):
+        r = np.zeros(3, np.float32)
+        l = np.zeros(3, np.float32)
+        N.lib().md_job_centers(self._h, N.fptr(r), N.fptr(l))
+        return r, l
+
+    def rotation_angles(self):
+        a = np.zeros(3 * self.n_rot, np.float32)
+        N.lib().md_job_rotation_angles(self._h, N.fptr(a))
+        return a.reshape(-1, 3)
+
+    def run(self, fft: FFTProcess | None = None):
+        rc = N.lib().md_job_run(self._h, fft._h if fft else None)
+        if rc:
+            raise MdError(rc, N.lib().md_job_error(self._h).decode())
+
+    def poses(self):
+        out = np.zeros(self.n_rot * self.t, POSE_DTYPE)
+        N.lib().md_job_poses(self._h, N.vptr(out))
+        return out
+
+    def top(self):
+        out = np.zeros(self.n_out, POSE_DTYPE)
+        N.lib().md_job_top(self._h, N.vptr(out))
+        return out
+
+    def close(self):
+        if getattr(self, "_h", None):
+            N.lib().md_job_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
