@@ -153,7 +153,32 @@ def run_reference_arm(args):
                                    f"OpenMP over all host cores)"},
         "e2e": {"value": value, "unit": "rotations/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
-    print(json.dumps(line))
+    print(json.dumps(line, default=float))
+
+
+def run_profile_case(args):
+    """A small batched run of the same workload for ncu: R rotations, one pass."""
+    import torch
+
+    from megadock_b200 import FFTProcess, Job, rotation_matrices
+    with tempfile.TemporaryDirectory() as tmp:
+        rp, lp = make_inputs(tmp)
+        job = Job(["-R", rp, "-L", lp, "-F", str(N_FFT), "-t", str(T_POSES), "-D", "-o",
+                   os.path.join(tmp, "p.out")])
+        mats = rotation_matrices(job.rotation_angles()[:args.profile_case])
+        fp = FFTProcess(0)
+        fp.alloc_array(job.nf1, job.grid_width, job.grid_coord())
+        rr, ri = job.receptor_grids()
+        fp.receptor_fft(rr, ri)
+        xyz, rad, q = job.ligand_atoms()
+        fp.ligand_data_transfer_gpu(xyz, rad, q, job.lig_core)
+        fp.set_batch(args.batch or 16)
+        d_rot = torch.from_numpy(mats).cuda()
+        d_pose = torch.zeros(len(mats) * T_POSES * 5, dtype=torch.int32, device="cuda")
+        fp.dock_profile(d_rot.data_ptr(), 0, len(mats), T_POSES, d_pose.data_ptr())
+        torch.cuda.synchronize()
+        fp.fft_memory_free()
+    print("profile case done")
 
 
 def main():
@@ -164,9 +189,13 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--batch", type=int, default=0, help="rotations per launch (0 = autotune)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-case", type=int, default=0, metavar="R",
+                    help="run R rotations of the batched form once (for ncu captures) and exit")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
+    if args.profile_case:
+        return run_profile_case(args)
 
     import numpy as np
     import torch
@@ -327,7 +356,7 @@ def main():
                                         "sample": f"{REF_SAMPLE_ROT} rotations of the same job ({secs:.1f} s)"}
         except Exception as e:  # the baseline is reported, never required
             line["cpu_baseline"] = {"error": str(e)[:200]}
-    print(json.dumps(line))
+    print(json.dumps(line, default=float))
     if dist:
         dist.destroy_process_group()
 
