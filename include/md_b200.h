@@ -99,6 +99,26 @@ int md_dock_profile(md_ctx *ctx, const float *d_rotmat, int first_rot, int n_rot
  * computed by the device voxelizer; grid_r/grid_i receive ng1^3 floats. */
 int md_ligand_voxels(md_ctx *ctx, const float *rotmat9, float *grid_r, float *grid_i);
 
+/* Allocation-free variant of md_dock_device.  No counterpart in the reference.
+ * For callers that cannot allocate device memory (a host framework whose pool
+ * allocator owns all device memory, a plugin that must not grow its host's
+ * footprint, a loop where cudaMalloc/cudaFree and their device-wide
+ * synchronisation are not allowed): every intermediate lives in one 32 MiB
+ * file-scope device array that each device loading the library holds until
+ * exit.  The caller passes all inputs and outputs as device pointers:
+ * grid_coord (ng1), receptor_spectrum (nf1^3 complex, interleaved re/im, as
+ * md_receptor_spectrum returns it), centred xyz (3*na), radius and charge (na),
+ * rotmat (9*n_rot), out (n_rot*t poses).  Limits: nf1 <= 128 with a built
+ * kernel set, na <= 32768, t <= 64 (else MD_ERR_SIZE); rotations run one per
+ * pipeline on `stream` (a cudaStream_t, NULL = default).  The first call on a
+ * device does the set-up with that device current: make it before any stream
+ * capture.  All calls share the one scratch array: calls that overlap on the
+ * GPU race, so the caller must serialise them.  Nothing is allocated, freed or
+ * synchronised; the call returns once the work is enqueued. */
+int md_dock_noalloc(int nf1, float grid_width, const float *d_grid_coord, const float *d_receptor_spectrum, int na,
+                    const float *d_xyz_centred, const float *d_radius, const float *d_charge, float lig_core,
+                    const float *d_rotmat, int first_rot, int n_rot, int t, md_pose *d_out, void *stream);
+
 /* ------------------------------------------------------------ host helpers */
 
 /* Rotation matrix of Docking::ligand_rotationz (src/docking.cpp:368-396) for

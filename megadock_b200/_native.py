@@ -52,6 +52,8 @@ _PROTOS = {
     "md_dock_device": (C.c_int, [_VP, _VP, C.c_int, C.c_int, C.c_int, _VP]),
     "md_ligand_voxels": (C.c_int, [_VP, _FP, _FP, _FP]),
     "md_dock_profile": (C.c_int, [_VP, _VP, C.c_int, C.c_int, C.c_int, _VP, _FP, _IP]),
+    "md_dock_noalloc": (C.c_int, [C.c_int, C.c_float, _VP, _VP, C.c_int, _VP, _VP, _VP, C.c_float, _VP, C.c_int,
+                                  C.c_int, C.c_int, _VP, _VP]),
     "md_rotation_matrix": (C.c_int, [_FP, _FP]),
     "md_sort_poses": (C.c_int, [_VP, C.c_int, C.c_int]),
     "md_job_create": (C.c_int, [C.c_int, C.POINTER(_CP), C.POINTER(_VP)]),

@@ -418,7 +418,7 @@ struct Cand {
 };
 
 // Block-wide best candidate strictly after (pk, pi) in selection order.
-__device__ Cand block_best(Cand mine, Cand *red) {
+__device__ __forceinline__ Cand block_best(Cand mine, Cand *red) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
@@ -549,7 +549,7 @@ __global__ void __launch_bounds__(kNT, 1)
 // ------------------------------------------------------------------ K4
 // Merge the N x t per-plane candidates of one rotation into t pose records
 // with the reference's rules (src/fft_process.cpp:408-458).
-__global__ void k_merge(const Cand *__restrict__ cand, int nplanes, int t, int N, float nf3f, int rot0,
+static __global__ void k_merge(const Cand *__restrict__ cand, int nplanes, int t, int N, float nf3f, int rot0,
                         DevPose *__restrict__ pose) {
     __shared__ Cand red[33];
     const int b = blockIdx.x;

@@ -1,0 +1,175 @@
+// md_dock_noalloc: the docking pipeline for callers that cannot allocate
+// device memory.
+//
+// Some callers of a docking library cannot call cudaMalloc: a host framework
+// that has already reserved all device memory for its own pool allocator, a
+// plugin that must not grow the process's footprint behind its host's back,
+// or a latency-critical loop where cudaMalloc/cudaFree (which synchronise the
+// device) are not allowed.  This entry point runs the same kernels as md_dock
+// but keeps every intermediate in one file-scope static device array, so it
+// calls no cudaMalloc, cudaFree or allocating library routine.  The caller
+// owns and passes all inputs and outputs as device pointers.
+//
+// Limits and rules:
+//   - scratch is kScratchBytes (32 MiB) per device, held by every device that
+//     loads the library until the process exits;
+//   - FFT edge nf1 <= 128 (nf1 must have a built kernel set), ligand atoms <=
+//     32768, t <= 64, and the per-rotation intermediates must fit the scratch;
+//     larger requests return MD_ERR_SIZE;
+//   - rotations run one per fused pipeline (the plain form);
+//   - the first call on each device does the set-up (symbol address lookup,
+//     twiddle tables, kernel attributes) with that device current; make that
+//     first call before any stream capture;
+//   - every call shares the one scratch array, which keeps the last call's
+//     contents: calls that overlap on the GPU (other streams, other threads)
+//     race and must be serialised by the caller.  No scratch region needs
+//     clearing: each stage fully overwrites its region before the next reads it.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <mutex>
+#include <vector>
+
+#include "../../include/md_b200.h"
+#include "dock_kernels.cuh"
+
+using namespace mdb;
+
+namespace {
+
+constexpr size_t kScratchBytes = size_t(32) << 20;
+constexpr int kMaxN = 128;
+constexpr int kMaxT = 64;
+constexpr int kMaxDevices = 64;
+// twiddle tables for every supported N <= kMaxN, concatenated
+constexpr int kTwSizes[] = {32, 48, 64, 80, 96, 112, 120, 128};
+constexpr int kTwTotal = 32 + 48 + 64 + 80 + 96 + 112 + 120 + 128;
+
+static __device__ __align__(256) unsigned char g_scratch[kScratchBytes];
+static __device__ __align__(256) float2 g_twiddle[kTwTotal];
+
+struct DevState {
+    bool ready = false;
+    unsigned char *scratch = nullptr;
+    float2 *twiddle = nullptr;
+};
+DevState g_state[kMaxDevices];
+std::mutex g_mu;
+
+int tw_offset(int n) {
+    int off = 0;
+    for (int s : kTwSizes) {
+        if (s == n) return off;
+        off += s;
+    }
+    return -1;
+}
+
+template <int N>
+cudaError_t set_attrs() {
+    const size_t plane = (size_t)N * (N + 1) * sizeof(float2);
+    const size_t fwd = plane + (kMaxLigAtoms / 32) * sizeof(uint32_t);
+    cudaError_t e = cudaFuncSetAttribute(k_plane_fwd<N, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fwd);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_plane_inv<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)plane);
+    return e;
+}
+
+// Once per device, with that device current.
+int setup(int dev) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    DevState &st = g_state[dev];
+    if (st.ready) return MD_OK;
+    void *p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_scratch) != cudaSuccess) return MD_ERR_CUDA;
+    st.scratch = static_cast<unsigned char *>(p);
+    if (cudaGetSymbolAddress(&p, g_twiddle) != cudaSuccess) return MD_ERR_CUDA;
+    st.twiddle = static_cast<float2 *>(p);
+    std::vector<float2> tw;
+    tw.reserve(kTwTotal);
+    for (int n : kTwSizes)
+        for (int j = 0; j < n; ++j) {
+            const double a = -2.0 * M_PI * (double)j / (double)n;
+            tw.push_back(make_float2((float)std::cos(a), (float)std::sin(a)));
+        }
+    if (cudaMemcpyToSymbol(g_twiddle, tw.data(), sizeof(float2) * kTwTotal) != cudaSuccess) return MD_ERR_CUDA;
+    cudaError_t e = cudaSuccess;
+#define X(n) \
+    if (e == cudaSuccess) e = set_attrs<n>();
+    X(32) X(48) X(64) X(80) X(96) X(112) X(120) X(128)
+#undef X
+    if (e != cudaSuccess) return MD_ERR_CUDA;
+    st.ready = true;
+    return MD_OK;
+}
+
+__global__ void k_pack_ligand(int na, const float *__restrict__ xyz, const float *__restrict__ radius,
+                              const float *__restrict__ charge, float4 *__restrict__ atom, float2 *__restrict__ rad2) {
+    const int l = blockIdx.x * blockDim.x + threadIdx.x;
+    if (l >= na) return;
+    atom[l] = make_float4(xyz[3 * l], xyz[3 * l + 1], xyz[3 * l + 2], charge[l]);
+    // R*R*1.5 and R*R*1.0 in float, as Ligand::precalc (src/ligand.cpp:251-254)
+    const float r = radius[l];
+    rad2[l] = make_float2(__fmul_rn(__fmul_rn(r, r), 1.5f), __fmul_rn(__fmul_rn(r, r), 1.0f));
+}
+
+template <int N>
+void run_rotation(cudaStream_t s, const LigandView &L, const GridView &G, const float *rot9, const float2 *Rh,
+                  float2 *A, float2 *Gsp, Cand *cand, int rot, int t, DevPose *pose) {
+    constexpr int NG = N / 2;
+    const size_t plane = (size_t)N * (N + 1) * sizeof(float2);
+    const size_t fwd = plane + (kMaxLigAtoms / 32) * sizeof(uint32_t);
+    const float nf3f = (float)((long long)N * N * N);
+    k_plane_fwd<N, 0><<<dim3(NG, 1), kNT, fwd, s>>>(L, G, rot9, nullptr, nullptr, A, nullptr, nullptr);
+    k_xline<N, 0><<<dim3(N * (N / kLT), 1), kNT, 0, s>>>(G, A, Rh, Gsp);
+    k_plane_inv<N><<<dim3(N, 1), kNT, plane, s>>>(G, Gsp, t, nf3f, cand);
+    k_merge<<<1, 256, 0, s>>>(cand, N, t, N, nf3f, rot, pose);
+}
+
+}  // namespace
+
+extern "C" int md_dock_noalloc(int nf1, float grid_width, const float *d_grid_coord, const float *d_receptor_spectrum,
+                               int na, const float *d_xyz_centred, const float *d_radius, const float *d_charge,
+                               float lig_core, const float *d_rotmat, int first_rot, int n_rot, int t,
+                               md_pose *d_out, void *stream) {
+    if (!d_grid_coord || !d_receptor_spectrum || !d_xyz_centred || !d_radius || !d_charge || !d_rotmat || !d_out)
+        return MD_ERR_ARG;
+    if (n_rot < 0 || t < 1 || na < 1 || !(grid_width > 0.f)) return MD_ERR_ARG;
+    if (lig_core == 0.0f || lig_core == -8888.0f) return MD_ERR_ARG;
+    if (nf1 > kMaxN || tw_offset(nf1) < 0 || t > kMaxT || na > kMaxLigAtoms) return MD_ERR_SIZE;
+    const size_t N = nf1, NG = nf1 / 2;
+    auto up = [](size_t b) { return (b + 255) & ~size_t(255); };
+    const size_t b_atom = up(sizeof(float4) * na), b_rad = up(sizeof(float2) * na);
+    const size_t b_A = up(sizeof(float2) * NG * N * N), b_G = up(sizeof(float2) * N * N * N);
+    const size_t b_cand = up(sizeof(Cand) * N * t);
+    if (b_atom + b_rad + b_A + b_G + b_cand > kScratchBytes) return MD_ERR_SIZE;
+    if (n_rot == 0) return MD_OK;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return MD_ERR_CUDA;
+    int rc = setup(dev);
+    if (rc) return rc;
+    const DevState &st = g_state[dev];
+    unsigned char *p = st.scratch;
+    float4 *atom = reinterpret_cast<float4 *>(p);
+    float2 *rad2 = reinterpret_cast<float2 *>(p + b_atom);
+    float2 *A = reinterpret_cast<float2 *>(p + b_atom + b_rad);
+    float2 *Gsp = reinterpret_cast<float2 *>(p + b_atom + b_rad + b_A);
+    Cand *cand = reinterpret_cast<Cand *>(p + b_atom + b_rad + b_A + b_G);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    k_pack_ligand<<<(na + 255) / 256, 256, 0, s>>>(na, d_xyz_centred, d_radius, d_charge, atom, rad2);
+    GridView G{(int)NG, grid_width, (float)((int)NG * grid_width) / 2, d_grid_coord, st.twiddle + tw_offset(nf1)};
+    LigandView L{na, atom, rad2, lig_core};
+    const float2 *Rh = reinterpret_cast<const float2 *>(d_receptor_spectrum);
+    DevPose *pose = reinterpret_cast<DevPose *>(d_out);
+    for (int r = 0; r < n_rot; ++r) {
+        const float *rot9 = d_rotmat + 9 * (size_t)r;
+        DevPose *pr = pose + (size_t)r * t;
+        switch (nf1) {
+#define X(n) \
+    case n: run_rotation<n>(s, L, G, rot9, Rh, A, Gsp, cand, first_rot + r, t, pr); break;
+            X(32) X(48) X(64) X(80) X(96) X(112) X(120) X(128)
+#undef X
+        }
+    }
+    return cudaGetLastError() == cudaSuccess ? MD_OK : MD_ERR_CUDA;
+}
