@@ -178,55 +178,66 @@ __device__ __forceinline__ float vox_real(const VoxShared<NG> &vs, int p, int q,
 
 // Charges of the atoms whose charge cell lies in plane p, added per cell in
 // ascending atom order starting from the cell's current value, exactly as the
-// sequential loop of src/ligand.cpp:216-234 rounds them.  `flags` is a bitmap
-// over atoms in shared memory; `cell(q, s)` returns a reference to the
-// cell's imaginary part.
+// sequential loop of src/ligand.cpp:216-234 rounds them.  Atoms are taken in
+// chunks of blockDim.x; each chunk's in-plane atoms are compacted in atom
+// order (warp ballots + a block prefix), then the first atom of every cell in
+// the chunk adds that cell's charges in order.  Chunks run in atom order.
+// `cell(q, s)` returns a reference to the cell's imaginary part.
+struct ChargeScratch {
+    int key[kNT];
+    float q[kNT];
+    int wsum[kNT / 32 + 1];
+};
+
 template <class Cell>
-__device__ void vox_charges(uint32_t *flags, const LigandView &L, const GridView &G, const float *m, int p,
+__device__ void vox_charges(ChargeScratch &cs, const LigandView &L, const GridView &G, const float *m, int p,
                             Cell cell) {
-    const int nw = (L.na + 31) >> 5;
-    for (int w = threadIdx.x; w < nw; w += blockDim.x) flags[w] = 0u;
-    __syncthreads();
-    for (int l = threadIdx.x; l < L.na; l += blockDim.x) {
-        const float4 a = __ldg(&L.atom[l]);
-        const float xr = rot_x(m, a.x, a.y, a.z);
-        if (charge_cell(xr, G.pad, G.gw, G.ng) == p) atomicOr(&flags[l >> 5], 1u << (l & 31));
-    }
-    __syncthreads();
-    if (threadIdx.x < 32) {
-        const int lane = threadIdx.x;
-        for (int w = 0; w < nw; ++w) {
-            const uint32_t word = flags[w];
-            if (!word) continue;
-            // lane i takes the i-th flagged atom of this word (ascending order)
-            int l = -1;
-            if (lane < __popc(word)) {
-                uint32_t x = word;
-                for (int s = 0; s < lane; ++s) x &= x - 1u;
-                l = (w << 5) + __ffs(x) - 1;
-            }
-            int key = -1;
-            float q = 0.f;
-            if (l >= 0) {
-                const float4 a = __ldg(&L.atom[l]);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+    for (int base = 0; base < L.na; base += blockDim.x) {
+        const int l = base + threadIdx.x;
+        bool in = false;
+        int key = 0;
+        float q = 0.f;
+        if (l < L.na) {
+            const float4 a = __ldg(&L.atom[l]);
+            if (charge_cell(rot_x(m, a.x, a.y, a.z), G.pad, G.gw, G.ng) == p) {
+                in = true;
                 const int j = charge_cell(rot_x(m + 3, a.x, a.y, a.z), G.pad, G.gw, G.ng);
                 const int k = charge_cell(rot_x(m + 6, a.x, a.y, a.z), G.pad, G.gw, G.ng);
                 key = j * G.ng + k;
                 q = a.w;
             }
-            const uint32_t grp = __match_any_sync(0xffffffffu, key);
-            const bool leader = (l >= 0) && (lane == __ffs(grp) - 1);
-            float acc = 0.f;
-            if (leader) acc = cell(key / G.ng, key % G.ng);
-            for (int b = 0; b < 32; ++b) {
-                const float qb = __shfl_sync(0xffffffffu, q, b);
-                if (leader && ((grp >> b) & 1u)) acc = __fadd_rn(acc, qb);
-            }
-            if (leader) cell(key / G.ng, key % G.ng) = acc;
-            __syncwarp();
         }
+        const uint32_t bal = __ballot_sync(0xffffffffu, in);
+        if (lane == 0) cs.wsum[warp] = __popc(bal);
+        __syncthreads();
+        int off = 0, total = 0;
+        for (int w = 0; w < nwarp; ++w) {
+            const int c = cs.wsum[w];
+            if (w < warp) off += c;
+            total += c;
+        }
+        if (in) {
+            const int pos = off + __popc(bal & ((1u << lane) - 1u));
+            cs.key[pos] = key;
+            cs.q[pos] = q;
+        }
+        __syncthreads();
+        if ((int)threadIdx.x < total) {
+            const int i = threadIdx.x;
+            const int ki = cs.key[i];
+            bool leader = true;
+            for (int j = 0; j < i && leader; ++j) leader = (cs.key[j] != ki);
+            if (leader) {
+                float &c = cell(ki / G.ng, ki % G.ng);
+                float acc = c;
+                for (int j = i; j < total; ++j)
+                    if (cs.key[j] == ki) acc = __fadd_rn(acc, cs.q[j]);
+                c = acc;
+            }
+        }
+        __syncthreads();
     }
-    __syncthreads();
 }
 
 // ------------------------------------------------------------------ K1
@@ -242,9 +253,9 @@ __global__ void __launch_bounds__(kNT, 1)
     constexpr int NG = N / 2, OFF = N / 4, PITCH = N + 1;
     constexpr int R1 = Plan<N>::R1, R2 = Plan<N>::R2;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    float2 *S = reinterpret_cast<float2 *>(smem_raw);                      // N x PITCH
-    uint32_t *flags = reinterpret_cast<uint32_t *>(S + (size_t)N * PITCH); // atom bitmap
+    float2 *S = reinterpret_cast<float2 *>(smem_raw);   // N x PITCH
     __shared__ VoxShared<NG> vs;
+    __shared__ ChargeScratch cs;
     __shared__ float m[9];
 
     const int p = blockIdx.x;
@@ -271,8 +282,7 @@ __global__ void __launch_bounds__(kNT, 1)
             S[(q + OFF) * PITCH + s + OFF] = make_float2(vox_real<NG>(vs, p, q, s, NG, L.delta, gd), 0.f);
         }
         __syncthreads();
-        vox_charges(flags, L, G, m, p,
-                    [&](int q, int s) -> float & { return S[(q + OFF) * PITCH + s + OFF].y; });
+        vox_charges(cs, L, G, m, p, [&](int q, int s) -> float & { return S[(q + OFF) * PITCH + s + OFF].y; });
         if (MODE == 2) {
             for (int c = tid; c < NG * NG; c += blockDim.x) {
                 const int q = c / NG, s = c % NG;
@@ -326,55 +336,110 @@ __global__ void __launch_bounds__(kNT, 1)
     }
 }
 
-// ------------------------------------------------------------------ K2
-// MODE 0: forward x-FFT, conj(R^) product, inverse x-FFT -> G.
-// MODE 1: forward x-FFT only -> R^ (receptor spectrum, written to `out`).
-template <int N, int MODE>
+// ------------------------------------------------------------------ K2 (receptor)
+// Forward x-FFT of the ng non-zero spectrum planes of the receptor: writes the
+// full receptor spectrum R^[kx][ky][kz].  CTA = (ky, 32 kz lines); the last
+// tile is partial when N is not a multiple of 32.
+template <int N>
 __global__ void __launch_bounds__(kNT)
-    k_xline(GridView G, const float2 *__restrict__ A, const float2 *__restrict__ Rh, float2 *__restrict__ out) {
+    k_xline_rec(GridView G, const float2 *__restrict__ A, float2 *__restrict__ Rh) {
     constexpr int NG = N / 2, OFF = N / 4;
     constexpr int R1 = Plan<N>::R1, R2 = Plan<N>::R2;
+    constexpr int TILES = (N + kLT - 1) / kLT;
     __shared__ float2 X[N * kLT];
-    const int lane = threadIdx.x & 31;
-    const int warp = threadIdx.x >> 5;
-    const int nwarp = blockDim.x >> 5;
-    constexpr int TILES = N / kLT;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
     const int ky = blockIdx.x / TILES;
-    const int kz0 = (blockIdx.x % TILES) * kLT;
-    const int b = blockIdx.y;
-
-    const float2 *Ab = A + (size_t)b * NG * N * N;
+    const int kz = (blockIdx.x % TILES) * kLT + lane;
+    const bool ok = kz < N;
     for (int pp = warp; pp < NG; pp += nwarp)
-        X[(pp + OFF) * kLT + lane] = Ab[((size_t)pp * N + ky) * N + kz0 + lane];
+        X[(pp + OFF) * kLT + lane] = ok ? A[((size_t)pp * N + ky) * N + kz] : make_float2(0.f, 0.f);
     __syncthreads();
     for (int it = threadIdx.x; it < kLT * R2; it += blockDim.x)
         fft_phase1<N, -1, true>(X + (it % kLT), kLT, it / kLT, G.tw);
     __syncthreads();
+    for (int it = threadIdx.x; it < kLT * R1; it += blockDim.x) {
+        const int ln = it % kLT, u = it / kLT;
+        float2 o[R2];
+        fft_phase2<N, -1>(X + ln, kLT, u, o);
+        if (ok)
+            static_for<0, R2>([&](auto k2) { Rh[((size_t)(u + R1 * k2) * N + ky) * N + kz] = o[k2]; });
+    }
+}
 
-    constexpr int IPT = (kLT * R1 + kNT - 1) / kNT;
-    if (MODE == 1) {
-        for (int it = threadIdx.x; it < kLT * R1; it += blockDim.x) {
-            const int ln = it % kLT, u = it / kLT;
-            float2 o[R2];
-            fft_phase2<N, -1>(X + ln, kLT, u, o);
-            static_for<0, R2>([&](auto k2) {
-                const int kx = u + R1 * k2;
-                out[((size_t)kx * N + ky) * N + kz0 + ln] = o[k2];
+// ------------------------------------------------------------------ K2 (docking)
+// The score grid s = IFFT(conj(R^) L^) is real, so only its Hermitian part
+//   H(k) = (P(k) + conj(P(-k))) / 2,   P = conj(R^) L^,
+// contributes: IFFT(H) = Re(IFFT(P)) exactly.  This kernel keeps the rows
+// ky in [1, N/2) of the x-inverted H and packs the two self-conjugate rows
+// ky = 0 and ky = N/2 into row 0 (row0 = g(ky=0) + i g(ky=N/2)); both become
+// real after the inverse along kz, so the plane kernel can unpack them.
+//
+// CTA = (ky in [0, N/2), 32 kz lines).  Per pass it loads the own tile
+// (ky, kz) and the mirror tile (-ky, -kz) straight from global memory into
+// the pruned forward x-FFT, multiplies both by conj(R^), folds the mirror into
+// H and runs the inverse x-FFT of the own tile.  CTAs of row 0 run two passes
+// (ky = 0 and ky = N/2) and pack them.  Output Gh[x][ky][kz], ky < N/2.
+template <int N>
+__global__ void __launch_bounds__(kNT)
+    k_xline_herm(GridView G, const float2 *__restrict__ A, const float2 *__restrict__ Rh, float2 *__restrict__ Gh) {
+    constexpr int NG = N / 2, NH = N / 2, OFF = N / 4;
+    constexpr int R1 = Plan<N>::R1, R2 = Plan<N>::R2;
+    constexpr int TILES = (N + kLT - 1) / kLT;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    float2 *X0 = reinterpret_cast<float2 *>(smem_raw);   // own tile   [N][kLT]
+    float2 *X1 = X0 + N * kLT;                           // mirror tile [N][kLT]
+    const int lane = threadIdx.x & 31;
+    const int ky = blockIdx.x / TILES;
+    const int kz = (blockIdx.x % TILES) * kLT + lane;
+    const bool ok = kz < N;
+    const int kzm = (N - kz) % N;
+    const int b = blockIdx.y;
+    const float2 *Ab = A + (size_t)b * NG * N * N;
+    float2 *Gb = Gh + (size_t)b * N * NH * N;
+    const int passes = (ky == 0) ? 2 : 1;
+
+    for (int pass = 0; pass < passes; ++pass) {
+        const int kyo = pass == 0 ? ky : NH;   // own row
+        const int kym = (N - kyo) % N;         // mirror row
+        // forward x pass 1 on both tiles, straight from global (pruned rows)
+        for (int it = threadIdx.x; it < 2 * kLT * R2; it += blockDim.x) {
+            const int s = it / (kLT * R2);
+            const int t = (it / kLT) % R2;
+            const int row = s ? kym : kyo, col = s ? kzm : kz;
+            float2 v[R1];
+            static_for<0, R1>([&](auto m_) {
+                constexpr int mm = decltype(m_)::value;
+                if constexpr (mm < R1 / 4 || mm >= 3 * R1 / 4) {
+                    v[mm] = make_float2(0.f, 0.f);
+                } else {
+                    const int pp = t + R2 * mm - OFF;
+                    v[mm] = ok ? Ab[((size_t)pp * N + row) * N + col] : make_float2(0.f, 0.f);
+                }
+            });
+            Dft<R1, -1>::run(v);
+            float2 *X = s ? X1 : X0;
+            static_for<0, R1>([&](auto k1_) {
+                constexpr int k1 = decltype(k1_)::value;
+                float2 x = v[k1];
+                if constexpr (k1 != 0) x = cmul(x, __ldg(&G.tw[t * k1]));
+                X[(k1 * R2 + t) * kLT + lane] = x;
             });
         }
-        return;
-    }
-    {
+        __syncthreads();
+        // forward x pass 2 and the conj(R^) product, held in registers
+        constexpr int IPT = (2 * kLT * R1 + kNT - 1) / kNT;
         float2 reg[IPT][R2];
 #pragma unroll
         for (int r = 0; r < IPT; ++r) {
-            const int it = threadIdx.x + r * blockDim.x;
-            if (it < kLT * R1) {
-                const int ln = it % kLT, u = it / kLT;
-                fft_phase2<N, -1>(X + ln, kLT, u, reg[r]);
+            const int it = threadIdx.x + r * kNT;
+            if (it < 2 * kLT * R1) {
+                const int s = it / (kLT * R1);
+                const int u = (it / kLT) % R1;
+                const int row = s ? kym : kyo, col = s ? kzm : kz;
+                fft_phase2<N, -1>((s ? X1 : X0) + lane, kLT, u, reg[r]);
                 static_for<0, R2>([&](auto k2) {
                     const int kx = u + R1 * k2;
-                    const float2 rh = __ldg(&Rh[((size_t)kx * N + ky) * N + kz0 + ln]);
+                    const float2 rh = ok ? __ldg(&Rh[((size_t)kx * N + row) * N + col]) : make_float2(0.f, 0.f);
                     reg[r][k2] = cmulconj(rh, reg[r][k2]);
                 });
             }
@@ -382,26 +447,55 @@ __global__ void __launch_bounds__(kNT)
         __syncthreads();
 #pragma unroll
         for (int r = 0; r < IPT; ++r) {
-            const int it = threadIdx.x + r * blockDim.x;
-            if (it < kLT * R1) {
-                const int ln = it % kLT, u = it / kLT;
-                static_for<0, R2>([&](auto k2) { X[(u + R1 * k2) * kLT + ln] = reg[r][k2]; });
+            const int it = threadIdx.x + r * kNT;
+            if (it < 2 * kLT * R1) {
+                const int s = it / (kLT * R1);
+                const int u = (it / kLT) % R1;
+                float2 *X = s ? X1 : X0;
+                static_for<0, R2>([&](auto k2) { X[(u + R1 * k2) * kLT + lane] = reg[r][k2]; });
             }
         }
-    }
-    __syncthreads();
-    for (int it = threadIdx.x; it < kLT * R2; it += blockDim.x)
-        fft_phase1<N, +1, false>(X + (it % kLT), kLT, it / kLT, G.tw);
-    __syncthreads();
-    float2 *Gb = out + (size_t)b * N * N * N;
-    for (int it = threadIdx.x; it < kLT * R1; it += blockDim.x) {
-        const int ln = it % kLT, u = it / kLT;
-        float2 o[R2];
-        fft_phase2<N, +1>(X + ln, kLT, u, o);
-        static_for<0, R2>([&](auto k2) {
-            const int x = u + R1 * k2;
-            Gb[((size_t)x * N + ky) * N + kz0 + ln] = o[k2];
-        });
+        __syncthreads();
+        // inverse x pass 1 of H = (P_own(kx) + conj(P_mirror(-kx))) / 2, in place in X0
+        for (int it = threadIdx.x; it < kLT * R2; it += blockDim.x) {
+            const int t = it / kLT;
+            float2 v[R1];
+            static_for<0, R1>([&](auto m_) {
+                constexpr int mm = decltype(m_)::value;
+                const int e = t + R2 * mm;
+                const float2 a = X0[e * kLT + lane];
+                const float2 c = X1[((N - e) % N) * kLT + lane];
+                v[mm] = make_float2(0.5f * (a.x + c.x), 0.5f * (a.y - c.y));
+            });
+            Dft<R1, +1>::run(v);
+            static_for<0, R1>([&](auto k1_) {
+                constexpr int k1 = decltype(k1_)::value;
+                float2 x = v[k1];
+                if constexpr (k1 != 0) x = cmul(x, conjf2(__ldg(&G.tw[t * k1])));
+                X0[(k1 * R2 + t) * kLT + lane] = x;
+            });
+        }
+        __syncthreads();
+        // inverse x pass 2 -> Gh (row 0 packs ky = 0 and ky = N/2)
+        for (int it = threadIdx.x; it < kLT * R1; it += blockDim.x) {
+            const int u = it / kLT;
+            float2 o[R2];
+            fft_phase2<N, +1>(X0 + lane, kLT, u, o);
+            if (ok) {
+                static_for<0, R2>([&](auto k2) {
+                    const int x = u + R1 * k2;
+                    float2 *dst = &Gb[((size_t)x * NH + ky) * N + kz];
+                    if (ky != 0 || pass == 0) {
+                        *dst = o[k2];
+                    } else {
+                        // same thread wrote the ky = 0 value in pass 0
+                        const float2 g0 = *dst;
+                        *dst = make_float2(g0.x - o[k2].y, g0.y + o[k2].x);
+                    }
+                });
+            }
+        }
+        __syncthreads();
     }
 }
 
@@ -417,7 +511,7 @@ struct Cand {
     int idx;
 };
 
-// Block-wide best candidate strictly after (pk, pi) in selection order.
+// Block-wide best candidate; idx < 0 means "none".
 __device__ __forceinline__ Cand block_best(Cand mine, Cand *red) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
@@ -451,98 +545,201 @@ __device__ __forceinline__ Cand block_best(Cand mine, Cand *red) {
     return r;
 }
 
-// Candidates are written as (key, linear index); key = raw real part when
-// t == 1 and raw / nf3 otherwise (src/fft_process.cpp:415, :437).
-template <int N>
-__global__ void __launch_bounds__(kNT, 1)
-    k_plane_inv(GridView G, const float2 *__restrict__ Gsp, int t, float nf3f, Cand *__restrict__ cand) {
-    constexpr int PITCH = N + 1;
+// Per-thread sorted list of the T best (key, index) pairs seen, best first.
+// Only candidates strictly after `floor` in selection order are kept (used
+// when a plane's top-t is found in several passes of T).
+template <int T>
+struct TopList {
+    float k[T];
+    int i[T];
+    __device__ __forceinline__ void init() {
+#pragma unroll
+        for (int j = 0; j < T; ++j) {
+            k[j] = 0.f;
+            i[j] = -1;
+        }
+    }
+    __device__ __forceinline__ void insert(float key, int idx, const Cand &floor) {
+        if (!(key == key)) return;   // NaN
+        if (floor.idx >= 0 && !key_better(floor.key, floor.idx, key, idx)) return;
+        if (i[T - 1] >= 0 && !key_better(key, idx, k[T - 1], i[T - 1])) return;
+#pragma unroll
+        for (int j = 0; j < T; ++j) {
+            if (i[j] < 0 || key_better(key, idx, k[j], i[j])) {
+                const float tk = k[j];
+                const int ti = i[j];
+                k[j] = key;
+                i[j] = idx;
+                key = tk;
+                idx = ti;
+                if (idx < 0) break;
+            }
+        }
+    }
+    __device__ __forceinline__ void pop() {
+#pragma unroll
+        for (int j = 0; j < T - 1; ++j) {
+            k[j] = k[j + 1];
+            i[j] = i[j + 1];
+        }
+        i[T - 1] = -1;
+    }
+};
+
+// K3: one x-plane of one rotation.  Input Gh[x][ky < N/2][kz] from
+// k_xline_herm.  (1) inverse FFT along kz of the N/2 rows, straight from
+// global memory; row 0 then holds h0 + i h_{N/2}, both real.  (2) complex-to-
+// real inverse along ky for every z column: with X the half spectrum,
+//   Z[k] = (X[k] + conj X[N/2-k]) + i w^k (X[k] - conj X[N/2-k]),  w = e^{2 pi i/N},
+// the N/2-point inverse FFT of Z gives s[2m] + i s[2m+1].  The scores feed a
+// per-thread top-T list directly (no score store), then a block merge writes
+// this plane's candidates cand[(b*N + x)*t + out0 + j] for j < nsel.
+// key = raw score when t == 1, raw / nf3 otherwise (src/fft_process.cpp:415, :437).
+template <int N, int T>
+__global__ void __launch_bounds__(kNT)
+    k_plane_c2r(GridView G, const float2 *__restrict__ Gh, int t, float nf3f, int out0, int nsel,
+                Cand *__restrict__ cand) {
+    constexpr int NH = N / 2;
     constexpr int R1 = Plan<N>::R1, R2 = Plan<N>::R2;
+    constexpr int Q1 = Plan<NH>::R1, Q2 = Plan<NH>::R2;
+    constexpr int PA = N + N / R2;   // step-1 layout: one pad per R2 block
+    constexpr int PB = N + 8;        // step-2 layout (natural order)
+    constexpr int PITCH = PA > PB ? PA : PB;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    float2 *S = reinterpret_cast<float2 *>(smem_raw);
-    float *SC = reinterpret_cast<float *>(smem_raw);
+    float2 *S = reinterpret_cast<float2 *>(smem_raw);   // NH x PITCH
     __shared__ Cand red[33];
     const int x = blockIdx.x;
     const int b = blockIdx.y;
     const int tid = threadIdx.x;
+    const float2 *Gp = Gh + ((size_t)b * N + x) * NH * N;
 
-    const float2 *Gp = Gsp + ((size_t)b * N + x) * N * N;
-    for (int e = tid; e < N * N; e += blockDim.x) S[(e / N) * PITCH + (e % N)] = Gp[e];
+    // (1a) inverse kz pass 1, straight from global: item = (row, t), t fastest
+    for (int it = tid; it < NH * R2; it += blockDim.x) {
+        const int row = it / R2, t = it % R2;
+        float2 v[R1];
+        static_for<0, R1>([&](auto m_) {
+            constexpr int mm = decltype(m_)::value;
+            v[mm] = __ldg(&Gp[(size_t)row * N + t + R2 * mm]);
+        });
+        Dft<R1, +1>::run(v);
+        static_for<0, R1>([&](auto k1_) {
+            constexpr int k1 = decltype(k1_)::value;
+            float2 xv = v[k1];
+            if constexpr (k1 != 0) xv = cmul(xv, conjf2(__ldg(&G.tw[t * k1])));
+            S[row * PITCH + k1 * (R2 + 1) + t] = xv;
+        });
+    }
     __syncthreads();
-    // inverse y: columns (lanes = kz)
-    for (int it = tid; it < N * R2; it += blockDim.x)
-        fft_phase1<N, +1, false>(S + (it % N), PITCH, it / N, G.tw);
-    __syncthreads();
-    constexpr int IPT = (N * R1 + kNT - 1) / kNT;
+    // (1b) inverse kz pass 2: item = (row, u), u fastest; natural order after a barrier
     {
+        constexpr int IPT = (NH * R1 + kNT - 1) / kNT;
         float2 reg[IPT][R2];
 #pragma unroll
         for (int r = 0; r < IPT; ++r) {
             const int it = tid + r * kNT;
-            if (it < N * R1) fft_phase2<N, +1>(S + (it % N), PITCH, it / N, reg[r]);
-        }
-        __syncthreads();
-#pragma unroll
-        for (int r = 0; r < IPT; ++r) {
-            const int it = tid + r * kNT;
-            if (it < N * R1) {
-                const int c = it % N, u = it / N;
-                static_for<0, R2>([&](auto k2) { S[(u + R1 * k2) * PITCH + c] = reg[r][k2]; });
-            }
-        }
-    }
-    __syncthreads();
-    // inverse z: rows (lanes = y)
-    for (int it = tid; it < N * R2; it += blockDim.x)
-        fft_phase1<N, +1, false>(S + (it % N) * PITCH, 1, it / N, G.tw);
-    __syncthreads();
-    {
-        float reg[IPT][R2];
-#pragma unroll
-        for (int r = 0; r < IPT; ++r) {
-            const int it = tid + r * kNT;
-            if (it < N * R1) {
-                float2 o[R2];
-                fft_phase2<N, +1>(S + (it % N) * PITCH, 1, it / N, o);
-                static_for<0, R2>([&](auto k2) {
-                    reg[r][k2] = (t == 1) ? o[k2].x : __fdiv_rn(o[k2].x, nf3f);
+            if (it < NH * R1) {
+                const int row = it / R1, u = it % R1;
+                static_for<0, R2>([&](auto n2_) {
+                    constexpr int n2 = decltype(n2_)::value;
+                    reg[r][n2] = S[row * PITCH + u * (R2 + 1) + n2];
                 });
+                Dft<R2, +1>::run(reg[r]);
             }
         }
         __syncthreads();
 #pragma unroll
         for (int r = 0; r < IPT; ++r) {
             const int it = tid + r * kNT;
-            if (it < N * R1) {
-                const int y = it % N, u = it / N;
-                static_for<0, R2>([&](auto k2) { SC[y * N + u + R1 * k2] = reg[r][k2]; });
+            if (it < NH * R1) {
+                const int row = it / R1, u = it % R1;
+                static_for<0, R2>([&](auto k2) { S[row * PITCH + u + R1 * k2] = reg[r][k2]; });
             }
         }
     }
     __syncthreads();
-    // t rounds of block-wide selection
-    Cand prev{0.f, -1};
-    Cand *out = cand + ((size_t)b * N + x) * t;
-    for (int round = 0; round < t; ++round) {
-        Cand mine{0.f, -1};
-        for (int e = tid; e < N * N; e += blockDim.x) {
-            const float k = SC[e];
-            if (!(k == k)) continue;   // NaN
-            const int idx = x * N * N + e;
-            if (prev.idx >= 0 && !key_better(prev.key, prev.idx, k, idx)) continue;
-            if (mine.idx < 0 || key_better(k, idx, mine.key, mine.idx)) {
-                mine.key = k;
-                mine.idx = idx;
+    // (2a) fold the half spectrum into Z, in place (pairs k, N/2-k)
+    for (int it = tid; it < N * (NH / 2 + 1); it += blockDim.x) {
+        const int z = it % N, k = it / N;
+        if (k == 0) {
+            const float2 v = S[z];   // X0 + i X_{N/2}, both real
+            S[z] = make_float2(v.x + v.y, v.x - v.y);
+        } else {
+            const int k2 = NH - k;
+            const float2 a = S[k * PITCH + z], c = S[k2 * PITCH + z];
+            const float2 wk = conjf2(__ldg(&G.tw[k])), wk2 = conjf2(__ldg(&G.tw[k2]));
+            // E = a + conj(c), D = a - conj(c), Z = E + i w^k D
+            const float2 e1 = make_float2(a.x + c.x, a.y - c.y), d1 = make_float2(a.x - c.x, a.y + c.y);
+            const float2 o1 = cmul(wk, d1);
+            const float2 z1 = make_float2(e1.x - o1.y, e1.y + o1.x);
+            if (k2 != k) {
+                const float2 e2 = make_float2(c.x + a.x, c.y - a.y), d2 = make_float2(c.x - a.x, c.y + a.y);
+                const float2 o2 = cmul(wk2, d2);
+                S[k2 * PITCH + z] = make_float2(e2.x - o2.y, e2.y + o2.x);
             }
+            S[k * PITCH + z] = z1;
         }
-        prev = block_best(mine, red);
-        if (tid == 0) out[round] = prev;
-        if (prev.idx < 0) {
-            // nothing left: fill the remaining slots as empty
+    }
+    __syncthreads();
+    // (2b) N/2-point inverse along ky, pass 1 (lanes = z), in place
+    for (int it = tid; it < N * Q2; it += blockDim.x) {
+        const int z = it % N, tt = it / N;
+        float2 v[Q1];
+        static_for<0, Q1>([&](auto m_) {
+            constexpr int mm = decltype(m_)::value;
+            v[mm] = S[(tt + Q2 * mm) * PITCH + z];
+        });
+        Dft<Q1, +1>::run(v);
+        static_for<0, Q1>([&](auto k1_) {
+            constexpr int k1 = decltype(k1_)::value;
+            float2 xv = v[k1];
+            if constexpr (k1 != 0) xv = cmul(xv, conjf2(__ldg(&G.tw[2 * tt * k1])));
+            S[(k1 * Q2 + tt) * PITCH + z] = xv;
+        });
+    }
+    __syncthreads();
+    // (2c) pass 2 -> scores s[2m], s[2m+1] -> per-thread top-T
+    TopList<T> top;
+    top.init();
+    Cand floor{0.f, -1};
+    Cand *out = cand + ((size_t)b * N + x) * t + out0;
+    if (out0 > 0) {
+        floor = out[-1];
+        if (floor.idx < 0) {   // an earlier pass already ran out of cells
             if (tid == 0)
-                for (int r2 = round + 1; r2 < t; ++r2) out[r2] = Cand{0.f, -1};
+                for (int r = 0; r < nsel; ++r) out[r] = Cand{0.f, -1};
+            return;
+        }
+    }
+    const int base = x * N * N;
+    for (int it = tid; it < N * Q1; it += blockDim.x) {
+        const int z = it % N, u = it / N;
+        float2 o[Q2];
+        static_for<0, Q2>([&](auto n2_) {
+            constexpr int n2 = decltype(n2_)::value;
+            o[n2] = S[(u * Q2 + n2) * PITCH + z];
+        });
+        Dft<Q2, +1>::run(o);
+        static_for<0, Q2>([&](auto k2_) {
+            constexpr int k2 = decltype(k2_)::value;
+            const int m2 = u + Q1 * k2;
+            const float se = o[k2].x, so = o[k2].y;
+            const float ke = (t == 1) ? se : __fdiv_rn(se, nf3f);
+            const float ko = (t == 1) ? so : __fdiv_rn(so, nf3f);
+            top.insert(ke, base + (2 * m2) * N + z, floor);
+            top.insert(ko, base + (2 * m2 + 1) * N + z, floor);
+        });
+    }
+    // block merge: nsel rounds over the per-thread heads
+    for (int r = 0; r < nsel; ++r) {
+        Cand mine{top.k[0], top.i[0]};
+        const Cand best = block_best(mine, red);
+        if (tid == 0) out[r] = best;
+        if (best.idx < 0) {
+            if (tid == 0)
+                for (int r2 = r + 1; r2 < nsel; ++r2) out[r2] = Cand{0.f, -1};
             break;
         }
+        if (top.i[0] == best.idx) top.pop();
     }
 }
 
@@ -550,7 +747,7 @@ __global__ void __launch_bounds__(kNT, 1)
 // Merge the N x t per-plane candidates of one rotation into t pose records
 // with the reference's rules (src/fft_process.cpp:408-458).
 static __global__ void k_merge(const Cand *__restrict__ cand, int nplanes, int t, int N, float nf3f, int rot0,
-                        DevPose *__restrict__ pose) {
+                               DevPose *__restrict__ pose) {
     __shared__ Cand red[33];
     const int b = blockIdx.x;
     const Cand *cb = cand + (size_t)b * nplanes * t;

@@ -202,9 +202,15 @@ struct Plan;
         static constexpr int R2 = R2_;                           \
         static_assert(R1_ * R2_ == N_ && R1_ % 4 == 0, "plan");  \
     };
+MDB_PLAN(16, 4, 4)
+MDB_PLAN(24, 4, 6)
 MDB_PLAN(32, 4, 8)
+MDB_PLAN(40, 8, 5)
 MDB_PLAN(48, 4, 12)
+MDB_PLAN(56, 8, 7)
+MDB_PLAN(60, 4, 15)
 MDB_PLAN(64, 8, 8)
+MDB_PLAN(72, 8, 9)
 MDB_PLAN(80, 8, 10)
 MDB_PLAN(96, 8, 12)
 MDB_PLAN(112, 8, 14)

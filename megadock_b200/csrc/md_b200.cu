@@ -47,7 +47,7 @@ struct md_ctx {
     int cap = 0;
     int cap_t = 0;
     float2 *d_A = nullptr;   // [cap][ng][N][N]
-    float2 *d_G = nullptr;   // [cap][N][N][N]
+    float2 *d_G = nullptr;   // [cap][N][N/2][N] (Hermitian half of the x-inverted product)
     Cand *d_cand = nullptr;  // [cap][N][t]
     // staging for host-buffer calls
     float *d_rot = nullptr;
@@ -75,27 +75,31 @@ namespace {
 template <int N>
 struct Sized {
     static constexpr int NG = N / 2;
-    static size_t smem_plane() { return (size_t)N * (N + 1) * sizeof(float2); }
-    static size_t smem_fwd() { return smem_plane() + (kMaxLigAtoms / 32) * sizeof(uint32_t); }
+    static constexpr int NH = N / 2;
+    static constexpr int TILES = (N + kLT - 1) / kLT;
+    static size_t smem_fwd() { return (size_t)N * (N + 1) * sizeof(float2); }
+    static size_t smem_xline() { return (size_t)2 * N * kLT * sizeof(float2); }
+    static size_t smem_c2r() {
+        constexpr int PA = N + Plan<N>::R1, PB = N + 8;
+        return (size_t)NH * (PA > PB ? PA : PB) * sizeof(float2);
+    }
 
     static cudaError_t set_attrs() {
         static bool done = false;
         if (done) return cudaSuccess;
-        cudaError_t e;
-        if ((e = cudaFuncSetAttribute(k_plane_fwd<N, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)smem_fwd())) != cudaSuccess)
-            return e;
-        if ((e = cudaFuncSetAttribute(k_plane_fwd<N, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)smem_fwd())) != cudaSuccess)
-            return e;
-        if ((e = cudaFuncSetAttribute(k_plane_fwd<N, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)smem_fwd())) != cudaSuccess)
-            return e;
-        if ((e = cudaFuncSetAttribute(k_plane_inv<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)smem_plane())) != cudaSuccess)
-            return e;
-        done = true;
-        return cudaSuccess;
+        cudaError_t e = cudaSuccess;
+        auto set = [&](const void *f, size_t bytes) {
+            if (e == cudaSuccess) e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+        };
+        set((const void *)k_plane_fwd<N, 0>, smem_fwd());
+        set((const void *)k_plane_fwd<N, 1>, smem_fwd());
+        set((const void *)k_plane_fwd<N, 2>, smem_fwd());
+        set((const void *)k_xline_herm<N>, smem_xline());
+        set((const void *)k_plane_c2r<N, 1>, smem_c2r());
+        set((const void *)k_plane_c2r<N, 4>, smem_c2r());
+        set((const void *)k_plane_c2r<N, 16>, smem_c2r());
+        if (e == cudaSuccess) done = true;
+        return e;
     }
 
     static void receptor(md_ctx *c, const float *d_r, const float *d_i) {
@@ -103,7 +107,7 @@ struct Sized {
         LigandView L{0, nullptr, nullptr, 1.f};
         k_plane_fwd<N, 1><<<dim3(NG, 1), kNT, smem_fwd(), c->stream>>>(L, G, nullptr, d_r, d_i, c->d_A, nullptr,
                                                                         nullptr);
-        k_xline<N, 1><<<dim3(N * (N / kLT), 1), kNT, 0, c->stream>>>(G, c->d_A, nullptr, c->d_Rh);
+        k_xline_rec<N><<<dim3(N * TILES, 1), kNT, 0, c->stream>>>(G, c->d_A, c->d_Rh);
     }
 
     static void voxels(md_ctx *c, const float *d_rot9, float *d_vr, float *d_vi) {
@@ -113,8 +117,22 @@ struct Sized {
                                                                         d_vi);
     }
 
+    // The plane top-t kernel in passes of T candidates (T = 1, 4 or 16).
+    static void plane_topt(cudaStream_t s, const GridView &G, const float2 *Gh, int nb, int t, float nf3f, Cand *cand) {
+        const int T = t == 1 ? 1 : (t <= 4 ? 4 : 16);
+        for (int out0 = 0; out0 < t; out0 += T) {
+            const int nsel = std::min(T, t - out0);
+            if (T == 1)
+                k_plane_c2r<N, 1><<<dim3(N, nb), kNT, smem_c2r(), s>>>(G, Gh, t, nf3f, out0, nsel, cand);
+            else if (T == 4)
+                k_plane_c2r<N, 4><<<dim3(N, nb), kNT, smem_c2r(), s>>>(G, Gh, t, nf3f, out0, nsel, cand);
+            else
+                k_plane_c2r<N, 16><<<dim3(N, nb), kNT, smem_c2r(), s>>>(G, Gh, t, nf3f, out0, nsel, cand);
+        }
+    }
+
     // One launch group: nb rotations whose matrices start at d_rot9.  With
-    // `ev` set, an event is recorded after each of the four kernels.
+    // `ev` set, an event is recorded after each of the four stages.
     static void dock(md_ctx *c, const float *d_rot9, int nb, int rot0, int t, DevPose *d_pose,
                      cudaEvent_t *ev = nullptr) {
         GridView G{c->ng, c->gw, (float)(c->ng * c->gw) / 2, c->d_gc, c->d_tw};
@@ -123,9 +141,9 @@ struct Sized {
         k_plane_fwd<N, 0><<<dim3(NG, nb), kNT, smem_fwd(), c->stream>>>(L, G, d_rot9, nullptr, nullptr, c->d_A,
                                                                          nullptr, nullptr);
         if (ev) cudaEventRecord(ev[1], c->stream);
-        k_xline<N, 0><<<dim3(N * (N / kLT), nb), kNT, 0, c->stream>>>(G, c->d_A, c->d_Rh, c->d_G);
+        k_xline_herm<N><<<dim3(NH * TILES, nb), kNT, smem_xline(), c->stream>>>(G, c->d_A, c->d_Rh, c->d_G);
         if (ev) cudaEventRecord(ev[2], c->stream);
-        k_plane_inv<N><<<dim3(N, nb), kNT, smem_plane(), c->stream>>>(G, c->d_G, t, nf3f, c->d_cand);
+        plane_topt(c->stream, G, c->d_G, nb, t, nf3f, c->d_cand);
         if (ev) cudaEventRecord(ev[3], c->stream);
         k_merge<<<nb, 256, 0, c->stream>>>(c->d_cand, N, t, N, nf3f, rot0, d_pose);
         if (ev) cudaEventRecord(ev[4], c->stream);
@@ -201,7 +219,7 @@ int ensure_work(md_ctx *ctx, int cap, int t) {
     cap = std::max(cap, 1);
     t = std::max(t, 1);
     MD_CUDA(cudaMalloc(&ctx->d_A, sizeof(float2) * cap * NG * N * N));
-    MD_CUDA(cudaMalloc(&ctx->d_G, sizeof(float2) * cap * N * N * N));
+    MD_CUDA(cudaMalloc(&ctx->d_G, sizeof(float2) * cap * N * (N / 2) * N));
     MD_CUDA(cudaMalloc(&ctx->d_cand, sizeof(Cand) * cap * N * t));
     ctx->cap = cap;
     ctx->cap_t = t;

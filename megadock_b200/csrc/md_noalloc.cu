@@ -66,12 +66,26 @@ int tw_offset(int n) {
 }
 
 template <int N>
+struct Smem {
+    static size_t fwd() { return (size_t)N * (N + 1) * sizeof(float2); }
+    static size_t xline() { return (size_t)2 * N * kLT * sizeof(float2); }
+    static size_t c2r() {
+        constexpr int PA = N + Plan<N>::R1, PB = N + 8;
+        return (size_t)(N / 2) * (PA > PB ? PA : PB) * sizeof(float2);
+    }
+};
+
+template <int N>
 cudaError_t set_attrs() {
-    const size_t plane = (size_t)N * (N + 1) * sizeof(float2);
-    const size_t fwd = plane + (kMaxLigAtoms / 32) * sizeof(uint32_t);
-    cudaError_t e = cudaFuncSetAttribute(k_plane_fwd<N, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fwd);
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(k_plane_inv<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)plane);
+    cudaError_t e = cudaSuccess;
+    auto set = [&](const void *f, size_t bytes) {
+        if (e == cudaSuccess) e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    };
+    set((const void *)k_plane_fwd<N, 0>, Smem<N>::fwd());
+    set((const void *)k_xline_herm<N>, Smem<N>::xline());
+    set((const void *)k_plane_c2r<N, 1>, Smem<N>::c2r());
+    set((const void *)k_plane_c2r<N, 4>, Smem<N>::c2r());
+    set((const void *)k_plane_c2r<N, 16>, Smem<N>::c2r());
     return e;
 }
 
@@ -116,13 +130,20 @@ __global__ void k_pack_ligand(int na, const float *__restrict__ xyz, const float
 template <int N>
 void run_rotation(cudaStream_t s, const LigandView &L, const GridView &G, const float *rot9, const float2 *Rh,
                   float2 *A, float2 *Gsp, Cand *cand, int rot, int t, DevPose *pose) {
-    constexpr int NG = N / 2;
-    const size_t plane = (size_t)N * (N + 1) * sizeof(float2);
-    const size_t fwd = plane + (kMaxLigAtoms / 32) * sizeof(uint32_t);
+    constexpr int NG = N / 2, NH = N / 2, TILES = (N + kLT - 1) / kLT;
     const float nf3f = (float)((long long)N * N * N);
-    k_plane_fwd<N, 0><<<dim3(NG, 1), kNT, fwd, s>>>(L, G, rot9, nullptr, nullptr, A, nullptr, nullptr);
-    k_xline<N, 0><<<dim3(N * (N / kLT), 1), kNT, 0, s>>>(G, A, Rh, Gsp);
-    k_plane_inv<N><<<dim3(N, 1), kNT, plane, s>>>(G, Gsp, t, nf3f, cand);
+    k_plane_fwd<N, 0><<<dim3(NG, 1), kNT, Smem<N>::fwd(), s>>>(L, G, rot9, nullptr, nullptr, A, nullptr, nullptr);
+    k_xline_herm<N><<<dim3(NH * TILES, 1), kNT, Smem<N>::xline(), s>>>(G, A, Rh, Gsp);
+    const int T = t == 1 ? 1 : (t <= 4 ? 4 : 16);
+    for (int out0 = 0; out0 < t; out0 += T) {
+        const int nsel = t - out0 < T ? t - out0 : T;
+        if (T == 1)
+            k_plane_c2r<N, 1><<<dim3(N, 1), kNT, Smem<N>::c2r(), s>>>(G, Gsp, t, nf3f, out0, nsel, cand);
+        else if (T == 4)
+            k_plane_c2r<N, 4><<<dim3(N, 1), kNT, Smem<N>::c2r(), s>>>(G, Gsp, t, nf3f, out0, nsel, cand);
+        else
+            k_plane_c2r<N, 16><<<dim3(N, 1), kNT, Smem<N>::c2r(), s>>>(G, Gsp, t, nf3f, out0, nsel, cand);
+    }
     k_merge<<<1, 256, 0, s>>>(cand, N, t, N, nf3f, rot, pose);
 }
 
@@ -140,7 +161,7 @@ extern "C" int md_dock_noalloc(int nf1, float grid_width, const float *d_grid_co
     const size_t N = nf1, NG = nf1 / 2;
     auto up = [](size_t b) { return (b + 255) & ~size_t(255); };
     const size_t b_atom = up(sizeof(float4) * na), b_rad = up(sizeof(float2) * na);
-    const size_t b_A = up(sizeof(float2) * NG * N * N), b_G = up(sizeof(float2) * N * N * N);
+    const size_t b_A = up(sizeof(float2) * NG * N * N), b_G = up(sizeof(float2) * N * (N / 2) * N);
     const size_t b_cand = up(sizeof(Cand) * N * t);
     if (b_atom + b_rad + b_A + b_G + b_cand > kScratchBytes) return MD_ERR_SIZE;
     if (n_rot == 0) return MD_OK;

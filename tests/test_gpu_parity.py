@@ -74,7 +74,9 @@ def test_device_voxels_vs_reference(built, gpu, pairs):
         assert np.array_equal(dr, rr) and np.array_equal(di, ri), r
 
 
-@pytest.mark.parametrize("name,extra", [("c0", ("-F", "96",)), ("c1", ("-F", "128",)), ("small", ("-F", "160",))])
+@pytest.mark.parametrize("name,extra", [("c0", ("-F", "96",)), ("c1", ("-F", "128",)), ("small", ("-F", "160",)),
+                                        ("small", ("-F", "80",)), ("small", ("-F", "112",)),
+                                        ("small", ("-F", "48", "-v", "2.0"))])
 def test_receptor_spectrum(built, gpu, pairs, name, extra):
     from oracle import oracle as O
     job, fp = _setup(pairs, name, *extra, "-r", "1")
@@ -109,6 +111,12 @@ def _check_rotation(got, rhat, job, r, t, m):
     ("c1", ("-F", "128", "-r", "54000"), 3, 12),
     ("small", ("-F", "64", "-r", "360"), 5, 30),
     ("small", ("-F", "160", "-r", "24"), 2, 4),
+    ("small", ("-F", "32", "-v", "3.0", "-r", "24"), 2, 8),
+    ("small", ("-F", "48", "-v", "2.0", "-r", "24"), 1, 8),
+    ("small", ("-F", "80", "-r", "360"), 4, 10),
+    ("small", ("-F", "112", "-r", "24"), 1, 6),
+    ("small", ("-F", "120", "-r", "24"), 17, 3),
+    ("small", ("-F", "144", "-r", "24"), 3, 4),
 ])
 def test_dock_matches_fp64_oracle(built, gpu, pairs, name, extra, t, nchk):
     from megadock_b200 import rotation_matrices
