@@ -88,52 +88,74 @@ __device__ __forceinline__ bool vbit(const uint32_t *plane, int q, int s) {
 }
 
 // Mark core / surface bits of planes around p for every atom near p.
+// Atoms are taken in chunks of blockDim.x: the chunk's atoms whose search box
+// reaches the planes of interest are compacted into `list` (any order -- the
+// marks are ORs), then every (atom, plane, row) of their boxes is one task,
+// spread evenly over the block; a task tests the row's cells and ORs the bits.
+struct MarkEntry {
+    float4 pos;   // rotated x, y, z and R^2 * 1.5
+    int4 box;     // search-box origin i, j, k and R^2 * 1.0 (as bits)
+};
+
 template <int NG>
-__device__ void vox_mark(VoxShared<NG> &vs, const LigandView &L, const GridView &G, const float *m, int p,
-                         bool general_delta) {
+__device__ void vox_mark(VoxShared<NG> &vs, MarkEntry *list, int *count, const LigandView &L, const GridView &G,
+                         const float *m, int p, bool general_delta) {
     constexpr int W = VoxShared<NG>::W;
     const int ng = G.ng;
     const int reach = general_delta ? 4 : 3;
-    const int plo = general_delta ? -2 : -1, phi = general_delta ? 2 : 1;
-    for (int l = threadIdx.x; l < L.na; l += blockDim.x) {
-        const float4 a = __ldg(&L.atom[l]);
-        const float xr = rot_x(m, a.x, a.y, a.z);
-        const int i2 = box_origin(xr, G.gw, ng);
-        if (i2 < p - reach || i2 > p + reach) continue;
-        const float yr = rot_x(m + 3, a.x, a.y, a.z);
-        const float zr = rot_x(m + 6, a.x, a.y, a.z);
-        const int j2 = box_origin(yr, G.gw, ng);
-        const int k2 = box_origin(zr, G.gw, ng);
-        const float2 r2 = __ldg(&L.rad2[l]);
-        const int ia = max(i2 - 2, max(0, p + plo)), ib = min(i2 + 3, min(ng, p + phi + 1));
-        const int ja = max(j2 - 2, 0), jb = min(j2 + 3, ng);
-        const int ka = max(k2 - 2, 0), kb = min(k2 + 3, ng);
-        for (int i = ia; i < ib; ++i) {
-            const float xd = sqdist(xr, __ldg(&G.gc[i]));
-            const int slot = i - p + 2;
-            const bool do_surf = (i >= p - 1 && i <= p + 1);
-            for (int j = ja; j < jb; ++j) {
-                const float d2 = __fadd_rn(xd, sqdist(yr, __ldg(&G.gc[j])));
-                uint32_t cbits[W], sbits[W];
-#pragma unroll
-                for (int w = 0; w < W; ++w) cbits[w] = sbits[w] = 0u;
-                for (int k = ka; k < kb; ++k) {
-                    const float d3 = __fadd_rn(d2, sqdist(zr, __ldg(&G.gc[k])));
-#pragma unroll
-                    for (int w = 0; w < W; ++w) {
-                        if ((k >> 5) == w) {
-                            if (d3 < r2.x) cbits[w] |= 1u << (k & 31);
-                            if (d3 < r2.y) sbits[w] |= 1u << (k & 31);
-                        }
-                    }
-                }
-#pragma unroll
-                for (int w = 0; w < W; ++w) {
-                    if (cbits[w]) atomicOr(&vs.core[slot][j * W + w], cbits[w]);
-                    if (do_surf && sbits[w]) atomicOr(&vs.surf[slot - 1][j * W + w], sbits[w]);
-                }
+    const int plo = general_delta ? -2 : -1;
+    const int nplanes = general_delta ? 5 : 3;
+    for (int base = 0; base < L.na; base += blockDim.x) {
+        if (threadIdx.x == 0) *count = 0;
+        __syncthreads();
+        const int l = base + threadIdx.x;
+        if (l < L.na) {
+            const float4 a = __ldg(&L.atom[l]);
+            const float xr = rot_x(m, a.x, a.y, a.z);
+            const int i2 = box_origin(xr, G.gw, ng);
+            if (i2 >= p - reach && i2 <= p + reach) {
+                const float yr = rot_x(m + 3, a.x, a.y, a.z);
+                const float zr = rot_x(m + 6, a.x, a.y, a.z);
+                const float2 r2 = __ldg(&L.rad2[l]);
+                const int slot = atomicAdd(count, 1);
+                list[slot].pos = make_float4(xr, yr, zr, r2.x);
+                list[slot].box = make_int4(i2, box_origin(yr, G.gw, ng), box_origin(zr, G.gw, ng), __float_as_int(r2.y));
             }
         }
+        __syncthreads();
+        const int ntask = *count * nplanes * 5;
+        for (int task = threadIdx.x; task < ntask; task += blockDim.x) {
+            const int e = task / (nplanes * 5);
+            const int rem = task % (nplanes * 5);
+            const int i = p + plo + rem / 5;
+            const MarkEntry me = list[e];
+            const int j = me.box.y - 2 + rem % 5;
+            if (i < 0 || i >= ng || i < me.box.x - 2 || i > me.box.x + 2 || j < 0 || j >= ng) continue;
+            const float rc2 = me.pos.w, rs2 = __int_as_float(me.box.w);
+            const float d2 = __fadd_rn(sqdist(me.pos.x, __ldg(&G.gc[i])), sqdist(me.pos.y, __ldg(&G.gc[j])));
+            uint32_t cbits[W], sbits[W];
+#pragma unroll
+            for (int w = 0; w < W; ++w) cbits[w] = sbits[w] = 0u;
+            const int ka = max(me.box.z - 2, 0), kb = min(me.box.z + 3, ng);
+            for (int k = ka; k < kb; ++k) {
+                const float d3 = __fadd_rn(d2, sqdist(me.pos.z, __ldg(&G.gc[k])));
+#pragma unroll
+                for (int w = 0; w < W; ++w) {
+                    if ((k >> 5) == w) {
+                        if (d3 < rc2) cbits[w] |= 1u << (k & 31);
+                        if (d3 < rs2) sbits[w] |= 1u << (k & 31);
+                    }
+                }
+            }
+            const int slot = i - p + 2;
+            const bool do_surf = (i >= p - 1 && i <= p + 1);
+#pragma unroll
+            for (int w = 0; w < W; ++w) {
+                if (cbits[w]) atomicOr(&vs.core[slot][j * W + w], cbits[w]);
+                if (do_surf && sbits[w]) atomicOr(&vs.surf[slot - 1][j * W + w], sbits[w]);
+            }
+        }
+        __syncthreads();
     }
 }
 
@@ -257,6 +279,7 @@ __global__ void __launch_bounds__(kNT, 1)
     __shared__ VoxShared<NG> vs;
     __shared__ ChargeScratch cs;
     __shared__ float m[9];
+    __shared__ int mark_count;
 
     const int p = blockIdx.x;
     const int b = blockIdx.y;
@@ -275,8 +298,9 @@ __global__ void __launch_bounds__(kNT, 1)
         for (int w = tid; w < 3 * NG * VoxShared<NG>::W; w += blockDim.x) (&vs.surf[0][0])[w] = 0u;
         __syncthreads();
         const bool gd = (L.delta != 1.0f);
-        vox_mark<NG>(vs, L, G, m, p, gd);
-        __syncthreads();
+        // the plane buffer is free until the voxel values are written: use it
+        // for the list of atoms near this plane
+        vox_mark<NG>(vs, reinterpret_cast<MarkEntry *>(S), &mark_count, L, G, m, p, gd);
         for (int c = tid; c < NG * NG; c += blockDim.x) {
             const int q = c / NG, s = c % NG;
             S[(q + OFF) * PITCH + s + OFF] = make_float2(vox_real<NG>(vs, p, q, s, NG, L.delta, gd), 0.f);
@@ -596,7 +620,7 @@ struct TopList {
 // this plane's candidates cand[(b*N + x)*t + out0 + j] for j < nsel.
 // key = raw score when t == 1, raw / nf3 otherwise (src/fft_process.cpp:415, :437).
 template <int N, int T>
-__global__ void __launch_bounds__(kNT)
+__global__ void __launch_bounds__(kNT, T <= 4 ? 3 : 2)
     k_plane_c2r(GridView G, const float2 *__restrict__ Gh, int t, float nf3f, int out0, int nsel,
                 Cand *__restrict__ cand) {
     constexpr int NH = N / 2;

@@ -77,7 +77,8 @@ struct Sized {
     static constexpr int NG = N / 2;
     static constexpr int NH = N / 2;
     static constexpr int TILES = (N + kLT - 1) / kLT;
-    static size_t smem_fwd() { return (size_t)N * (N + 1) * sizeof(float2); }
+    // the plane buffer also holds the voxelizer's atom list (kNT entries)
+    static size_t smem_fwd() { return std::max((size_t)N * (N + 1) * sizeof(float2), kNT * sizeof(MarkEntry)); }
     static size_t smem_xline() { return (size_t)2 * N * kLT * sizeof(float2); }
     static size_t smem_c2r() {
         constexpr int PA = N + Plan<N>::R1, PB = N + 8;

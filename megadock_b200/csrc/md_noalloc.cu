@@ -67,7 +67,10 @@ int tw_offset(int n) {
 
 template <int N>
 struct Smem {
-    static size_t fwd() { return (size_t)N * (N + 1) * sizeof(float2); }
+    static size_t fwd() {
+        const size_t plane = (size_t)N * (N + 1) * sizeof(float2), list = kNT * sizeof(MarkEntry);
+        return plane > list ? plane : list;
+    }
     static size_t xline() { return (size_t)2 * N * kLT * sizeof(float2); }
     static size_t c2r() {
         constexpr int PA = N + Plan<N>::R1, PB = N + 8;
