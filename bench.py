@@ -43,6 +43,7 @@ T_POSES = 3
 ROT_SET = 54000
 METRIC = "rotations/sec at 128^3, 54k rot: batched vs plain fused, same GPU, 1e-4 tol"
 REF_SAMPLE_ROT = 360
+PLAIN_SAMPLE = 5400
 
 
 def _peaks():
@@ -264,9 +265,15 @@ def main():
         fp.set_batch(batch)
         with Clocks(local) as clk:
             ms_batched = timed(dev_step, args.steps, args.warmup)
-        # plain form (one rotation per pipeline)
+        # plain form (one rotation per pipeline, no graph): its per-rotation
+        # cost does not depend on the rotation count, so it is timed on the
+        # first PLAIN_SAMPLE rotations of the set
         fp.set_batch(1)
-        ms_plain = timed(dev_step, max(1, args.steps // 2), 1)
+
+        def plain_step():
+            fp.dock_device(d_rot.data_ptr(), 0, PLAIN_SAMPLE, T_POSES, d_pose.data_ptr())
+
+        ms_plain = timed(plain_step, args.steps, 1) * nrot / PLAIN_SAMPLE
         # e2e through the C ABI with host buffers
         fp.set_batch(batch)
         host_rot = np.ascontiguousarray(mats)
@@ -299,15 +306,18 @@ def main():
 
     N3 = N_FFT ** 3
     nb_launches = -(-nrot // batch)
-    # algorithmic bytes per rotation per stage (complex64 = 8 B)
+    # algorithmic DRAM bytes per rotation per stage (complex64 = 8 B, NG = N/2)
+    NG = N_FFT // 2
     stage_bytes = {
-        "plane_fwd": 8 * N3 // 2,            # write the ng non-zero spectrum planes
-        "xline": 8 * N3 // 2 + 8 * N3,       # read them, write the product after the inverse x pass
-        "plane_inv": 8 * N3,                 # read the x-inverted spectrum once
+        "voxelize": NG ** 3 // 4,                    # two class bit planes per voxel plane
+        "plane_fwd": NG ** 3 // 4 + 4 * N3,           # read them, write ng spectrum planes (N^2 each)
+        "xline": 4 * N3 + 4 * N3,                     # read those, write the Hermitian half (N/2 rows)
+        "plane_inv": 4 * N3,                          # read the half once
         "merge": 0,
     }
-    names = ["plane_fwd", "xline", "plane_inv", "merge"]
-    dom = max(range(4), key=lambda k: stage_ms[k])
+    names = ["voxelize", "plane_fwd", "xline", "plane_inv", "merge"]
+    dom = max(range(5), key=lambda k: stage_ms[k])
+    # R^ is read once per launch (it is shared by the launch's rotations)
     dom_bytes_launch = stage_bytes[names[dom]] * batch + (8 * N3 if names[dom] == "xline" else 0)
     dom_ms_launch = stage_ms[dom] / nb_launches
     peak, peak_kind = _peaks()
@@ -331,7 +341,8 @@ def main():
                    "fft": N_FFT, "rotations": ROT_SET, "t": T_POSES, "rotations_per_launch": batch,
                    "l2": "working set per step >> L2 (54,000 rotations x ~25 MB of intermediates)",
                    "parallelism": f"replicas x{world}"},
-        "plain": {"value": plain, "ms_per_step": ms_plain, "unit": "rotations/s"},
+        "plain": {"value": plain, "ms_per_step": ms_plain, "unit": "rotations/s",
+                  "sample": f"first {PLAIN_SAMPLE} rotations per step, scaled to {ROT_SET}"},
         "batched_over_plain": value / plain,
         "e2e": {"value": e2e, "unit": "rotations/s", "ms_per_step": ms_e2e,
                 "h2d_bytes_per_step": int(rr.nbytes + ri.nbytes + mats.nbytes + xyz.nbytes + rad.nbytes + q.nbytes),
@@ -339,10 +350,11 @@ def main():
         "roofline": {"bound": "hbm", "kernel": names[dom], "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
                      "stage_ms": {n: float(stage_ms[k]) for k, n in enumerate(names)}},
+        "pipeline_bytes_per_rotation": {"model_52N3": model_bytes, "this_pipeline": sum(stage_bytes.values())},
         "pipeline_model": {"bytes_per_rotation": model_bytes,
                            "achieved_GBps": model_bytes * value / 1e9,
                            "frac": model_bytes * value / 1e9 / peak},
-        "gpu_launches": int(args.steps * 4 * nb_launches),
+        "gpu_launches": int(args.steps * 5 * nb_launches),
         "clocks": clk.summary(),
     }
     if not args.no_cpu_baseline:

@@ -87,11 +87,12 @@ int md_dock(md_ctx *ctx, const float *rotmat, int first_rot, int n_rot, int t, m
 /* Same with device-resident rotation matrices and device output buffer. */
 int md_dock_device(md_ctx *ctx, const float *d_rotmat, int first_rot, int n_rot, int t, md_pose *d_out);
 
-/* Per-stage device time of md_dock_device's launches (no graph): stage_ms[4]
- * receives the summed CUDA-event time of the rotate+voxelize+forward-plane
- * kernel, the x-line product kernel, the inverse-plane top-t kernel and the
- * merge kernel; *launches the number of kernel launches.  Replaces the
- * reference's gettimeofday buckets (src/cpu_time.h:35-61). */
+/* Per-stage device time of md_dock_device's launches (no graph): stage_ms[5]
+ * receives the summed CUDA-event time of the voxelizer (rotation, rPSC classes
+ * and ordered charge sums), the forward-plane kernel (y/z FFT), the x-line
+ * product kernel, the inverse-plane top-t kernel and the merge kernel;
+ * *launches the number of kernel launches.  Replaces the reference's
+ * gettimeofday buckets (src/cpu_time.h:35-61). */
 int md_dock_profile(md_ctx *ctx, const float *d_rotmat, int first_rot, int n_rot, int t, md_pose *d_out,
                     float *stage_ms, int *launches);
 

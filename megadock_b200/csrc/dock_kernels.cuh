@@ -178,24 +178,21 @@ __device__ __forceinline__ int vox_class(const VoxShared<NG> &vs, int slot, int 
     return vbit<NG>(vs.surf[slot - 1], q, s) ? 1 : 0;
 }
 
-// Real rPSC value of cell (p, q, s).
+// Real rPSC class of cell (p, q, s): 2 = core (value delta), 1 = surface
+// (value 1.0), 0 = empty.  With delta != 1 the interior core cells next to an
+// empty cell become surface (src/ligand.cpp:176-195).
 template <int NG>
-__device__ __forceinline__ float vox_real(const VoxShared<NG> &vs, int p, int q, int s, int ng, float delta,
-                                          bool general_delta) {
+__device__ __forceinline__ int vox_code(const VoxShared<NG> &vs, int p, int q, int s, int ng, bool general_delta) {
     const int c = vox_class<NG>(vs, 2, p, q, s, ng);
-    if (c == 1) return 1.0f;
-    if (c == 0) return 0.0f;
-    if (general_delta) {
-        // src/ligand.cpp:176-195: interior core cells next to an empty cell -> 1.0
-        const bool interior = p >= 1 && p <= ng - 2 && q >= 1 && q <= ng - 2 && s >= 1 && s <= ng - 2;
-        if (interior) {
-            if (vox_class<NG>(vs, 1, p - 1, q, s, ng) == 0 || vox_class<NG>(vs, 3, p + 1, q, s, ng) == 0 ||
-                vox_class<NG>(vs, 2, p, q - 1, s, ng) == 0 || vox_class<NG>(vs, 2, p, q + 1, s, ng) == 0 ||
-                vox_class<NG>(vs, 2, p, q, s - 1, ng) == 0 || vox_class<NG>(vs, 2, p, q, s + 1, ng) == 0)
-                return 1.0f;
-        }
+    if (c != 2 || !general_delta) return c;
+    const bool interior = p >= 1 && p <= ng - 2 && q >= 1 && q <= ng - 2 && s >= 1 && s <= ng - 2;
+    if (interior) {
+        if (vox_class<NG>(vs, 1, p - 1, q, s, ng) == 0 || vox_class<NG>(vs, 3, p + 1, q, s, ng) == 0 ||
+            vox_class<NG>(vs, 2, p, q - 1, s, ng) == 0 || vox_class<NG>(vs, 2, p, q + 1, s, ng) == 0 ||
+            vox_class<NG>(vs, 2, p, q, s - 1, ng) == 0 || vox_class<NG>(vs, 2, p, q, s + 1, ng) == 0)
+            return 1;
     }
-    return delta;
+    return 2;
 }
 
 // Charges of the atoms whose charge cell lies in plane p, added per cell in
@@ -262,24 +259,81 @@ __device__ void vox_charges(ChargeScratch &cs, const LigandView &L, const GridVi
     }
 }
 
-// ------------------------------------------------------------------ K1
-// MODE 0: ligand rotation + voxelization, store spectrum planes A.
-// MODE 1: receptor grids (re, im) loaded from global, store spectrum planes A.
-// MODE 2: ligand rotation + voxelization, store the voxel plane itself
-//         (ng x ng real and imaginary parts) for parity checks; no FFT.
-template <int N, int MODE>
-__global__ void __launch_bounds__(kNT, 1)
-    k_plane_fwd(LigandView L, GridView G, const float *__restrict__ rotm, const float *__restrict__ src_r,
-                const float *__restrict__ src_i, float2 *__restrict__ A, float *__restrict__ vox_r,
-                float *__restrict__ vox_i) {
-    constexpr int NG = N / 2, OFF = N / 4, PITCH = N + 1;
-    constexpr int R1 = Plan<N>::R1, R2 = Plan<N>::R2;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    float2 *S = reinterpret_cast<float2 *>(smem_raw);   // N x PITCH
+// ------------------------------------------------------------------ K0
+// Ligand grid of one (rotation, x-plane p), everything but the FFT:
+//  * real part: core / surface marks of the atoms near p (task-parallel), the
+//    swollen-surface scrape and the surface fill (src/ligand.cpp:20-198),
+//    stored as two bit planes: vbits[b][p][0] = "value delta",
+//    vbits[b][p][1] = "value 1.0";
+//  * imaginary part: the per-cell charge sums in ascending atom order
+//    (src/ligand.cpp:200-239), stored as a compact list of the plane's charged
+//    cells qlist[b][p][e] = (q * NG + s, sum as bits), qcount[b][p] entries.
+constexpr int kNT0 = 256;
+
+template <int NG>
+__global__ void __launch_bounds__(kNT0)
+    k_vox_bits(LigandView L, GridView G, const float *__restrict__ rotm, uint32_t *__restrict__ vbits,
+               int2 *__restrict__ qlist, int *__restrict__ qcount) {
+    constexpr int W = VoxShared<NG>::W;
     __shared__ VoxShared<NG> vs;
+    __shared__ MarkEntry list[kNT0];
+    __shared__ uint32_t ob[2][NG * W];
+    __shared__ float qplane[NG * NG];
+    __shared__ uint32_t touched[NG * W];
     __shared__ ChargeScratch cs;
     __shared__ float m[9];
-    __shared__ int mark_count;
+    __shared__ int count;
+    const int p = blockIdx.x, b = blockIdx.y, tid = threadIdx.x;
+    if (tid < 9) m[tid] = rotm[(size_t)b * 9 + tid];
+    for (int w = tid; w < 5 * NG * W; w += blockDim.x) (&vs.core[0][0])[w] = 0u;
+    for (int w = tid; w < 3 * NG * W; w += blockDim.x) (&vs.surf[0][0])[w] = 0u;
+    for (int w = tid; w < 2 * NG * W; w += blockDim.x) (&ob[0][0])[w] = 0u;
+    for (int w = tid; w < NG * W; w += blockDim.x) touched[w] = 0u;
+    for (int c = tid; c < NG * NG; c += blockDim.x) qplane[c] = 0.f;
+    __syncthreads();
+    const bool gd = (L.delta != 1.0f);
+    vox_mark<NG>(vs, list, &count, L, G, m, p, gd);
+    for (int c = tid; c < NG * NG; c += blockDim.x) {
+        const int q = c / NG, s2 = c % NG;
+        const int code = vox_code<NG>(vs, p, q, s2, NG, gd);
+        if (code) atomicOr(&ob[2 - code][q * W + (s2 >> 5)], 1u << (s2 & 31));
+    }
+    vox_charges(cs, L, G, m, p, [&](int q, int s2) -> float & {
+        atomicOr(&touched[q * W + (s2 >> 5)], 1u << (s2 & 31));
+        return qplane[q * NG + s2];
+    });
+    // vox_charges ends with a barrier
+    uint32_t *dst = vbits + ((size_t)b * NG + p) * 2 * NG * W;
+    for (int w = tid; w < 2 * NG * W; w += blockDim.x) dst[w] = (&ob[0][0])[w];
+    if (tid == 0) count = 0;
+    __syncthreads();
+    int2 *ql = qlist + ((size_t)b * NG + p) * NG * NG;
+    for (int c = tid; c < NG * NG; c += blockDim.x) {
+        const int q = c / NG, s2 = c % NG;
+        if ((touched[q * W + (s2 >> 5)] >> (s2 & 31)) & 1u) {
+            const int e = atomicAdd(&count, 1);
+            ql[e] = make_int2(c, __float_as_int(qplane[c]));
+        }
+    }
+    __syncthreads();
+    if (tid == 0) qcount[(size_t)b * NG + p] = count;
+}
+
+// ------------------------------------------------------------------ K1
+// MODE 0: real part from the K0 bit planes + K0 charge list, store spectrum planes A.
+// MODE 1: receptor grids (re, im) loaded from global, store spectrum planes A.
+// MODE 2: like MODE 0 but store the voxel plane itself (ng x ng real and
+//         imaginary parts) for parity checks; no FFT.
+template <int N, int MODE>
+__global__ void __launch_bounds__(kNT, 1)
+    k_plane_fwd(LigandView L, GridView G, const uint32_t *__restrict__ vbits, const int2 *__restrict__ qlist,
+                const int *__restrict__ qcount, const float *__restrict__ src_r, const float *__restrict__ src_i,
+                float2 *__restrict__ A, float *__restrict__ vox_r, float *__restrict__ vox_i) {
+    constexpr int NG = N / 2, OFF = N / 4, PITCH = N + 1;
+    constexpr int R1 = Plan<N>::R1, R2 = Plan<N>::R2;
+    constexpr int W = VoxShared<NG>::W;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    float2 *S = reinterpret_cast<float2 *>(smem_raw);   // N x PITCH
 
     const int p = blockIdx.x;
     const int b = blockIdx.y;
@@ -293,20 +347,22 @@ __global__ void __launch_bounds__(kNT, 1)
         }
         __syncthreads();
     } else {
-        if (tid < 9) m[tid] = rotm[(size_t)b * 9 + tid];
-        for (int w = tid; w < 5 * NG * VoxShared<NG>::W; w += blockDim.x) (&vs.core[0][0])[w] = 0u;
-        for (int w = tid; w < 3 * NG * VoxShared<NG>::W; w += blockDim.x) (&vs.surf[0][0])[w] = 0u;
-        __syncthreads();
-        const bool gd = (L.delta != 1.0f);
-        // the plane buffer is free until the voxel values are written: use it
-        // for the list of atoms near this plane
-        vox_mark<NG>(vs, reinterpret_cast<MarkEntry *>(S), &mark_count, L, G, m, p, gd);
+        const uint32_t *vb = vbits + ((size_t)b * NG + p) * 2 * NG * W;
         for (int c = tid; c < NG * NG; c += blockDim.x) {
             const int q = c / NG, s = c % NG;
-            S[(q + OFF) * PITCH + s + OFF] = make_float2(vox_real<NG>(vs, p, q, s, NG, L.delta, gd), 0.f);
+            const uint32_t bit = 1u << (s & 31);
+            const float v = (__ldg(&vb[q * W + (s >> 5)]) & bit) ? L.delta
+                            : (__ldg(&vb[NG * W + q * W + (s >> 5)]) & bit) ? 1.0f : 0.0f;
+            S[(q + OFF) * PITCH + s + OFF] = make_float2(v, 0.f);
         }
         __syncthreads();
-        vox_charges(cs, L, G, m, p, [&](int q, int s) -> float & { return S[(q + OFF) * PITCH + s + OFF].y; });
+        const int nq = qcount[(size_t)b * NG + p];
+        const int2 *ql = qlist + ((size_t)b * NG + p) * NG * NG;
+        for (int e = tid; e < nq; e += blockDim.x) {
+            const int2 c = ql[e];
+            S[(c.x / NG + OFF) * PITCH + c.x % NG + OFF].y = __int_as_float(c.y);
+        }
+        __syncthreads();
         if (MODE == 2) {
             for (int c = tid; c < NG * NG; c += blockDim.x) {
                 const int q = c / NG, s = c % NG;

@@ -49,6 +49,9 @@ struct md_ctx {
     float2 *d_A = nullptr;   // [cap][ng][N][N]
     float2 *d_G = nullptr;   // [cap][N][N/2][N] (Hermitian half of the x-inverted product)
     Cand *d_cand = nullptr;  // [cap][N][t]
+    uint32_t *d_vbits = nullptr;   // [cap][N/2][2][N/2 * words per row] voxel class bit planes
+    int2 *d_qlist = nullptr;       // [cap][N/2][(N/2)^2] charged cells of each voxel plane
+    int *d_qcount = nullptr;       // [cap][N/2]
     // staging for host-buffer calls
     float *d_rot = nullptr;
     size_t rot_cap = 0;
@@ -77,8 +80,7 @@ struct Sized {
     static constexpr int NG = N / 2;
     static constexpr int NH = N / 2;
     static constexpr int TILES = (N + kLT - 1) / kLT;
-    // the plane buffer also holds the voxelizer's atom list (kNT entries)
-    static size_t smem_fwd() { return std::max((size_t)N * (N + 1) * sizeof(float2), kNT * sizeof(MarkEntry)); }
+    static size_t smem_fwd() { return (size_t)N * (N + 1) * sizeof(float2); }
     static size_t smem_xline() { return (size_t)2 * N * kLT * sizeof(float2); }
     static size_t smem_c2r() {
         constexpr int PA = N + Plan<N>::R1, PB = N + 8;
@@ -106,16 +108,17 @@ struct Sized {
     static void receptor(md_ctx *c, const float *d_r, const float *d_i) {
         GridView G{c->ng, c->gw, 0.f, c->d_gc, c->d_tw};
         LigandView L{0, nullptr, nullptr, 1.f};
-        k_plane_fwd<N, 1><<<dim3(NG, 1), kNT, smem_fwd(), c->stream>>>(L, G, nullptr, d_r, d_i, c->d_A, nullptr,
-                                                                        nullptr);
+        k_plane_fwd<N, 1><<<dim3(NG, 1), kNT, smem_fwd(), c->stream>>>(L, G, nullptr, nullptr, nullptr, d_r, d_i,
+                                                                        c->d_A, nullptr, nullptr);
         k_xline_rec<N><<<dim3(N * TILES, 1), kNT, 0, c->stream>>>(G, c->d_A, c->d_Rh);
     }
 
     static void voxels(md_ctx *c, const float *d_rot9, float *d_vr, float *d_vi) {
         GridView G{c->ng, c->gw, (float)(c->ng * c->gw) / 2, c->d_gc, c->d_tw};
         LigandView L{c->na, c->d_atom, c->d_rad2, c->delta};
-        k_plane_fwd<N, 2><<<dim3(NG, 1), kNT, smem_fwd(), c->stream>>>(L, G, d_rot9, nullptr, nullptr, nullptr, d_vr,
-                                                                        d_vi);
+        k_vox_bits<NG><<<dim3(NG, 1), kNT0, 0, c->stream>>>(L, G, d_rot9, c->d_vbits, c->d_qlist, c->d_qcount);
+        k_plane_fwd<N, 2><<<dim3(NG, 1), kNT, smem_fwd(), c->stream>>>(L, G, c->d_vbits, c->d_qlist, c->d_qcount,
+                                                                        nullptr, nullptr, nullptr, d_vr, d_vi);
     }
 
     // The plane top-t kernel in passes of T candidates (T = 1, 4 or 16).
@@ -133,21 +136,23 @@ struct Sized {
     }
 
     // One launch group: nb rotations whose matrices start at d_rot9.  With
-    // `ev` set, an event is recorded after each of the four stages.
+    // `ev` set, an event is recorded after each of the five stages.
     static void dock(md_ctx *c, const float *d_rot9, int nb, int rot0, int t, DevPose *d_pose,
                      cudaEvent_t *ev = nullptr) {
         GridView G{c->ng, c->gw, (float)(c->ng * c->gw) / 2, c->d_gc, c->d_tw};
         LigandView L{c->na, c->d_atom, c->d_rad2, c->delta};
         const float nf3f = (float)((long long)N * N * N);
-        k_plane_fwd<N, 0><<<dim3(NG, nb), kNT, smem_fwd(), c->stream>>>(L, G, d_rot9, nullptr, nullptr, c->d_A,
-                                                                         nullptr, nullptr);
+        k_vox_bits<NG><<<dim3(NG, nb), kNT0, 0, c->stream>>>(L, G, d_rot9, c->d_vbits, c->d_qlist, c->d_qcount);
         if (ev) cudaEventRecord(ev[1], c->stream);
-        k_xline_herm<N><<<dim3(NH * TILES, nb), kNT, smem_xline(), c->stream>>>(G, c->d_A, c->d_Rh, c->d_G);
+        k_plane_fwd<N, 0><<<dim3(NG, nb), kNT, smem_fwd(), c->stream>>>(L, G, c->d_vbits, c->d_qlist, c->d_qcount,
+                                                                         nullptr, nullptr, c->d_A, nullptr, nullptr);
         if (ev) cudaEventRecord(ev[2], c->stream);
-        plane_topt(c->stream, G, c->d_G, nb, t, nf3f, c->d_cand);
+        k_xline_herm<N><<<dim3(NH * TILES, nb), kNT, smem_xline(), c->stream>>>(G, c->d_A, c->d_Rh, c->d_G);
         if (ev) cudaEventRecord(ev[3], c->stream);
-        k_merge<<<nb, 256, 0, c->stream>>>(c->d_cand, N, t, N, nf3f, rot0, d_pose);
+        plane_topt(c->stream, G, c->d_G, nb, t, nf3f, c->d_cand);
         if (ev) cudaEventRecord(ev[4], c->stream);
+        k_merge<<<nb, 256, 0, c->stream>>>(c->d_cand, N, t, N, nf3f, rot0, d_pose);
+        if (ev) cudaEventRecord(ev[5], c->stream);
     }
 };
 
@@ -212,9 +217,15 @@ int ensure_work(md_ctx *ctx, int cap, int t) {
     cudaFree(ctx->d_A);
     cudaFree(ctx->d_G);
     cudaFree(ctx->d_cand);
+    cudaFree(ctx->d_vbits);
+    cudaFree(ctx->d_qlist);
+    cudaFree(ctx->d_qcount);
     ctx->d_A = nullptr;
     ctx->d_G = nullptr;
     ctx->d_cand = nullptr;
+    ctx->d_vbits = nullptr;
+    ctx->d_qlist = nullptr;
+    ctx->d_qcount = nullptr;
     ctx->cap = ctx->cap_t = 0;
     const size_t N = ctx->N, NG = ctx->ng;
     cap = std::max(cap, 1);
@@ -222,6 +233,9 @@ int ensure_work(md_ctx *ctx, int cap, int t) {
     MD_CUDA(cudaMalloc(&ctx->d_A, sizeof(float2) * cap * NG * N * N));
     MD_CUDA(cudaMalloc(&ctx->d_G, sizeof(float2) * cap * N * (N / 2) * N));
     MD_CUDA(cudaMalloc(&ctx->d_cand, sizeof(Cand) * cap * N * t));
+    MD_CUDA(cudaMalloc(&ctx->d_vbits, sizeof(uint32_t) * cap * NG * 2 * NG * ((NG + 31) / 32)));
+    MD_CUDA(cudaMalloc(&ctx->d_qlist, sizeof(int2) * cap * NG * NG * NG));
+    MD_CUDA(cudaMalloc(&ctx->d_qcount, sizeof(int) * cap * NG));
     ctx->cap = cap;
     ctx->cap_t = t;
     return MD_OK;
@@ -319,6 +333,9 @@ void md_ctx_destroy(md_ctx *ctx) {
     cudaFree(ctx->d_A);
     cudaFree(ctx->d_G);
     cudaFree(ctx->d_cand);
+    cudaFree(ctx->d_vbits);
+    cudaFree(ctx->d_qlist);
+    cudaFree(ctx->d_qcount);
     cudaFree(ctx->d_rot);
     cudaFree(ctx->d_pose);
     if (ctx->own) cudaStreamDestroy(ctx->own);
@@ -350,6 +367,12 @@ int md_set_grid(md_ctx *ctx, int nf1, float grid_width, const float *grid_coord)
         cudaFree(ctx->d_A);
         cudaFree(ctx->d_G);
         cudaFree(ctx->d_cand);
+        cudaFree(ctx->d_vbits);
+        cudaFree(ctx->d_qlist);
+        cudaFree(ctx->d_qcount);
+        ctx->d_vbits = nullptr;
+        ctx->d_qlist = nullptr;
+        ctx->d_qcount = nullptr;
         ctx->d_gc = nullptr;
         ctx->d_tw = nullptr;
         ctx->d_Rh = nullptr;
@@ -511,25 +534,25 @@ int md_dock_profile(md_ctx *ctx, const float *d_rot, int first_rot, int n_rot, i
     MD_CUDA(cudaSetDevice(ctx->device));
     const int B = std::max(1, std::min(ctx->batch, n_rot));
     if ((rc = ensure_work(ctx, B, t))) return rc;
-    cudaEvent_t ev[5];
+    cudaEvent_t ev[6];
     for (auto &e : ev) MD_CUDA(cudaEventCreate(&e));
-    double acc[4] = {0, 0, 0, 0};
+    double acc[5] = {0, 0, 0, 0, 0};
     int nl = 0;
     for (int r = 0; r < n_rot; r += B) {
         const int nb = std::min(B, n_rot - r);
         MD_CUDA(cudaEventRecord(ev[0], ctx->stream));
         launch_dock(ctx, d_rot + 9 * (size_t)r, nb, first_rot + r, t,
                     reinterpret_cast<DevPose *>(d_out) + (size_t)r * t, ev);
-        nl += 4;
-        MD_CUDA(cudaEventSynchronize(ev[4]));
-        for (int k = 0; k < 4; ++k) {
+        nl += 5;
+        MD_CUDA(cudaEventSynchronize(ev[5]));
+        for (int k = 0; k < 5; ++k) {
             float ms = 0.f;
             MD_CUDA(cudaEventElapsedTime(&ms, ev[k], ev[k + 1]));
             acc[k] += ms;
         }
     }
     for (auto &e : ev) cudaEventDestroy(e);
-    for (int k = 0; k < 4; ++k) stage_ms[k] = (float)acc[k];
+    for (int k = 0; k < 5; ++k) stage_ms[k] = (float)acc[k];
     if (launches) *launches = nl;
     MD_CUDA(cudaGetLastError());
     return MD_OK;

@@ -67,10 +67,7 @@ int tw_offset(int n) {
 
 template <int N>
 struct Smem {
-    static size_t fwd() {
-        const size_t plane = (size_t)N * (N + 1) * sizeof(float2), list = kNT * sizeof(MarkEntry);
-        return plane > list ? plane : list;
-    }
+    static size_t fwd() { return (size_t)N * (N + 1) * sizeof(float2); }
     static size_t xline() { return (size_t)2 * N * kLT * sizeof(float2); }
     static size_t c2r() {
         constexpr int PA = N + Plan<N>::R1, PB = N + 8;
@@ -132,10 +129,13 @@ __global__ void k_pack_ligand(int na, const float *__restrict__ xyz, const float
 
 template <int N>
 void run_rotation(cudaStream_t s, const LigandView &L, const GridView &G, const float *rot9, const float2 *Rh,
-                  float2 *A, float2 *Gsp, Cand *cand, int rot, int t, DevPose *pose) {
+                  uint32_t *vbits, int2 *qlist, int *qcount, float2 *A, float2 *Gsp, Cand *cand, int rot, int t,
+                  DevPose *pose) {
     constexpr int NG = N / 2, NH = N / 2, TILES = (N + kLT - 1) / kLT;
     const float nf3f = (float)((long long)N * N * N);
-    k_plane_fwd<N, 0><<<dim3(NG, 1), kNT, Smem<N>::fwd(), s>>>(L, G, rot9, nullptr, nullptr, A, nullptr, nullptr);
+    k_vox_bits<NG><<<dim3(NG, 1), kNT0, 0, s>>>(L, G, rot9, vbits, qlist, qcount);
+    k_plane_fwd<N, 0><<<dim3(NG, 1), kNT, Smem<N>::fwd(), s>>>(L, G, vbits, qlist, qcount, nullptr, nullptr, A,
+                                                               nullptr, nullptr);
     k_xline_herm<N><<<dim3(NH * TILES, 1), kNT, Smem<N>::xline(), s>>>(G, A, Rh, Gsp);
     const int T = t == 1 ? 1 : (t <= 4 ? 4 : 16);
     for (int out0 = 0; out0 < t; out0 += T) {
@@ -166,7 +166,9 @@ extern "C" int md_dock_noalloc(int nf1, float grid_width, const float *d_grid_co
     const size_t b_atom = up(sizeof(float4) * na), b_rad = up(sizeof(float2) * na);
     const size_t b_A = up(sizeof(float2) * NG * N * N), b_G = up(sizeof(float2) * N * (N / 2) * N);
     const size_t b_cand = up(sizeof(Cand) * N * t);
-    if (b_atom + b_rad + b_A + b_G + b_cand > kScratchBytes) return MD_ERR_SIZE;
+    const size_t b_bits = up(sizeof(uint32_t) * NG * 2 * NG * ((NG + 31) / 32));
+    const size_t b_ql = up(sizeof(int2) * NG * NG * NG), b_qc = up(sizeof(int) * NG);
+    if (b_atom + b_rad + b_A + b_G + b_cand + b_bits + b_ql + b_qc > kScratchBytes) return MD_ERR_SIZE;
     if (n_rot == 0) return MD_OK;
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return MD_ERR_CUDA;
@@ -179,6 +181,9 @@ extern "C" int md_dock_noalloc(int nf1, float grid_width, const float *d_grid_co
     float2 *A = reinterpret_cast<float2 *>(p + b_atom + b_rad);
     float2 *Gsp = reinterpret_cast<float2 *>(p + b_atom + b_rad + b_A);
     Cand *cand = reinterpret_cast<Cand *>(p + b_atom + b_rad + b_A + b_G);
+    uint32_t *vbits = reinterpret_cast<uint32_t *>(p + b_atom + b_rad + b_A + b_G + b_cand);
+    int2 *qlist = reinterpret_cast<int2 *>(p + b_atom + b_rad + b_A + b_G + b_cand + b_bits);
+    int *qcount = reinterpret_cast<int *>(p + b_atom + b_rad + b_A + b_G + b_cand + b_bits + b_ql);
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     k_pack_ligand<<<(na + 255) / 256, 256, 0, s>>>(na, d_xyz_centred, d_radius, d_charge, atom, rad2);
     GridView G{(int)NG, grid_width, (float)((int)NG * grid_width) / 2, d_grid_coord, st.twiddle + tw_offset(nf1)};
@@ -190,7 +195,7 @@ extern "C" int md_dock_noalloc(int nf1, float grid_width, const float *d_grid_co
         DevPose *pr = pose + (size_t)r * t;
         switch (nf1) {
 #define X(n) \
-    case n: run_rotation<n>(s, L, G, rot9, Rh, A, Gsp, cand, first_rot + r, t, pr); break;
+    case n: run_rotation<n>(s, L, G, rot9, Rh, vbits, qlist, qcount, A, Gsp, cand, first_rot + r, t, pr); break;
             X(32) X(48) X(64) X(80) X(96) X(112) X(120) X(128)
 #undef X
         }

@@ -80,8 +80,9 @@ class FFTProcess:
                self._h)
 
     def dock_profile(self, d_rotmat: int, first_rot: int, n_rot: int, t: int, d_out: int):
-        """Per-stage device milliseconds (4 stages) and the launch count."""
-        ms = np.zeros(4, np.float32)
+        """Per-stage device milliseconds (voxelize, plane_fwd, xline, plane_inv,
+        merge) and the launch count."""
+        ms = np.zeros(5, np.float32)
         nl = C.c_int()
         _check(N.lib().md_dock_profile(self._h, C.c_void_p(d_rotmat), first_rot, n_rot, t, C.c_void_p(d_out),
                                        N.fptr(ms), C.byref(nl)), self._h)
