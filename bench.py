@@ -354,7 +354,7 @@ def main():
         "pipeline_model": {"bytes_per_rotation": model_bytes,
                            "achieved_GBps": model_bytes * value / 1e9,
                            "frac": model_bytes * value / 1e9 / peak},
-        "gpu_launches": int(args.steps * 5 * nb_launches),
+        "gpu_launches": int(args.steps * launches_prof),
         "clocks": clk.summary(),
     }
     if not args.no_cpu_baseline:

@@ -87,76 +87,62 @@ __device__ __forceinline__ bool vbit(const uint32_t *plane, int q, int s) {
     return (plane[q * W + (s >> 5)] >> (s & 31)) & 1u;
 }
 
-// Mark core / surface bits of planes around p for every atom near p.
-// Atoms are taken in chunks of blockDim.x: the chunk's atoms whose search box
-// reaches the planes of interest are compacted into `list` (any order -- the
-// marks are ORs), then every (atom, plane, row) of their boxes is one task,
-// spread evenly over the block; a task tests the row's cells and ORs the bits.
+// Per-rotation atom record for the voxelizer: rotated coordinates, the
+// search-box origin (src/ligand.cpp:71-73) and both sphere radii squared.
 struct MarkEntry {
     float4 pos;   // rotated x, y, z and R^2 * 1.5
     int4 box;     // search-box origin i, j, k and R^2 * 1.0 (as bits)
 };
 
+// Shape buckets: atoms are grouped by box origin i, shifted by kReach so that
+// origins in [-kReach, ng + kReach) map to [0, ng + 2 kReach).
+constexpr int kReach = 4;
+
+// Mark core / surface bits of the planes around p.  The atoms whose box can
+// reach those planes are the contiguous bucket range [lo, hi) of the rotation's
+// record array; every (atom, plane, row) of their boxes is one task, spread
+// evenly over the block; a task tests the row's cells and ORs the bits (the
+// marks are ORs, so the order of atoms does not matter).
 template <int NG>
-__device__ void vox_mark(VoxShared<NG> &vs, MarkEntry *list, int *count, const LigandView &L, const GridView &G,
-                         const float *m, int p, bool general_delta) {
+__device__ void vox_mark(VoxShared<NG> &vs, const MarkEntry *__restrict__ rec, int lo, int hi, const GridView &G,
+                         int p, bool general_delta) {
     constexpr int W = VoxShared<NG>::W;
     const int ng = G.ng;
-    const int reach = general_delta ? 4 : 3;
     const int plo = general_delta ? -2 : -1;
     const int nplanes = general_delta ? 5 : 3;
-    for (int base = 0; base < L.na; base += blockDim.x) {
-        if (threadIdx.x == 0) *count = 0;
-        __syncthreads();
-        const int l = base + threadIdx.x;
-        if (l < L.na) {
-            const float4 a = __ldg(&L.atom[l]);
-            const float xr = rot_x(m, a.x, a.y, a.z);
-            const int i2 = box_origin(xr, G.gw, ng);
-            if (i2 >= p - reach && i2 <= p + reach) {
-                const float yr = rot_x(m + 3, a.x, a.y, a.z);
-                const float zr = rot_x(m + 6, a.x, a.y, a.z);
-                const float2 r2 = __ldg(&L.rad2[l]);
-                const int slot = atomicAdd(count, 1);
-                list[slot].pos = make_float4(xr, yr, zr, r2.x);
-                list[slot].box = make_int4(i2, box_origin(yr, G.gw, ng), box_origin(zr, G.gw, ng), __float_as_int(r2.y));
-            }
-        }
-        __syncthreads();
-        const int ntask = *count * nplanes * 5;
-        for (int task = threadIdx.x; task < ntask; task += blockDim.x) {
-            const int e = task / (nplanes * 5);
-            const int rem = task % (nplanes * 5);
-            const int i = p + plo + rem / 5;
-            const MarkEntry me = list[e];
-            const int j = me.box.y - 2 + rem % 5;
-            if (i < 0 || i >= ng || i < me.box.x - 2 || i > me.box.x + 2 || j < 0 || j >= ng) continue;
-            const float rc2 = me.pos.w, rs2 = __int_as_float(me.box.w);
-            const float d2 = __fadd_rn(sqdist(me.pos.x, __ldg(&G.gc[i])), sqdist(me.pos.y, __ldg(&G.gc[j])));
-            uint32_t cbits[W], sbits[W];
+    const int ntask = (hi - lo) * nplanes * 5;
+    for (int task = threadIdx.x; task < ntask; task += blockDim.x) {
+        const int e = task / (nplanes * 5);
+        const int rem = task % (nplanes * 5);
+        const int i = p + plo + rem / 5;
+        const MarkEntry me = rec[lo + e];
+        const int j = me.box.y - 2 + rem % 5;
+        if (i < 0 || i >= ng || i < me.box.x - 2 || i > me.box.x + 2 || j < 0 || j >= ng) continue;
+        const float rc2 = me.pos.w, rs2 = __int_as_float(me.box.w);
+        const float d2 = __fadd_rn(sqdist(me.pos.x, __ldg(&G.gc[i])), sqdist(me.pos.y, __ldg(&G.gc[j])));
+        uint32_t cbits[W], sbits[W];
 #pragma unroll
-            for (int w = 0; w < W; ++w) cbits[w] = sbits[w] = 0u;
-            const int ka = max(me.box.z - 2, 0), kb = min(me.box.z + 3, ng);
-            for (int k = ka; k < kb; ++k) {
-                const float d3 = __fadd_rn(d2, sqdist(me.pos.z, __ldg(&G.gc[k])));
-#pragma unroll
-                for (int w = 0; w < W; ++w) {
-                    if ((k >> 5) == w) {
-                        if (d3 < rc2) cbits[w] |= 1u << (k & 31);
-                        if (d3 < rs2) sbits[w] |= 1u << (k & 31);
-                    }
-                }
-            }
-            const int slot = i - p + 2;
-            const bool do_surf = (i >= p - 1 && i <= p + 1);
+        for (int w = 0; w < W; ++w) cbits[w] = sbits[w] = 0u;
+        const int ka = max(me.box.z - 2, 0), kb = min(me.box.z + 3, ng);
+        for (int k = ka; k < kb; ++k) {
+            const float d3 = __fadd_rn(d2, sqdist(me.pos.z, __ldg(&G.gc[k])));
 #pragma unroll
             for (int w = 0; w < W; ++w) {
-                if (cbits[w]) atomicOr(&vs.core[slot][j * W + w], cbits[w]);
-                if (do_surf && sbits[w]) atomicOr(&vs.surf[slot - 1][j * W + w], sbits[w]);
+                if ((k >> 5) == w) {
+                    if (d3 < rc2) cbits[w] |= 1u << (k & 31);
+                    if (d3 < rs2) sbits[w] |= 1u << (k & 31);
+                }
             }
         }
-        __syncthreads();
+        const int slot = i - p + 2;
+        const bool do_surf = (i >= p - 1 && i <= p + 1);
+#pragma unroll
+        for (int w = 0; w < W; ++w) {
+            if (cbits[w]) atomicOr(&vs.core[slot][j * W + w], cbits[w]);
+            if (do_surf && sbits[w]) atomicOr(&vs.surf[slot - 1][j * W + w], sbits[w]);
+        }
     }
+    __syncthreads();
 }
 
 // Core bit survives the swollen-surface scrape (src/ligand.cpp:110-134):
@@ -195,67 +181,95 @@ __device__ __forceinline__ int vox_code(const VoxShared<NG> &vs, int p, int q, i
     return 2;
 }
 
-// Charges of the atoms whose charge cell lies in plane p, added per cell in
-// ascending atom order starting from the cell's current value, exactly as the
-// sequential loop of src/ligand.cpp:216-234 rounds them.  Atoms are taken in
-// chunks of blockDim.x; each chunk's in-plane atoms are compacted in atom
-// order (warp ballots + a block prefix), then the first atom of every cell in
-// the chunk adds that cell's charges in order.  Chunks run in atom order.
-// `cell(q, s)` returns a reference to the cell's imaginary part.
-struct ChargeScratch {
-    int key[kNT];
-    float q[kNT];
-    int wsum[kNT / 32 + 1];
-};
+// ------------------------------------------------------------------ atom prep
+// Once per rotation: rotate every atom (src/docking.cpp:386-393), compute its
+// search-box origin and its charge cell (src/ligand.cpp:71-73, 219-221) and
+// bucket the atoms by x-plane:
+//  * shape records rec[b][.] grouped by box origin i (any order inside a
+//    bucket), bucket starts sstart[b][0 .. ng + 2 kReach];
+//  * charge entries cq[b][.] = (cell j * ng + k, charge bits) grouped by the
+//    charge cell's plane, in ascending atom order inside a bucket (the order
+//    in which MEGADOCK adds charges), bucket starts cstart[b][0 .. ng].
+constexpr int kNTP = 256;
 
-template <class Cell>
-__device__ void vox_charges(ChargeScratch &cs, const LigandView &L, const GridView &G, const float *m, int p,
-                            Cell cell) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
-    for (int base = 0; base < L.na; base += blockDim.x) {
-        const int l = base + threadIdx.x;
-        bool in = false;
-        int key = 0;
-        float q = 0.f;
-        if (l < L.na) {
-            const float4 a = __ldg(&L.atom[l]);
-            if (charge_cell(rot_x(m, a.x, a.y, a.z), G.pad, G.gw, G.ng) == p) {
-                in = true;
-                const int j = charge_cell(rot_x(m + 3, a.x, a.y, a.z), G.pad, G.gw, G.ng);
-                const int k = charge_cell(rot_x(m + 6, a.x, a.y, a.z), G.pad, G.gw, G.ng);
-                key = j * G.ng + k;
+template <int NG>
+__global__ void __launch_bounds__(kNTP)
+    k_atom_prep(LigandView L, GridView G, const float *__restrict__ rotm, MarkEntry *__restrict__ rec,
+                int *__restrict__ sstart, int2 *__restrict__ cq, int *__restrict__ cstart) {
+    constexpr int NBS = NG + 2 * kReach;
+    __shared__ int cnt_s[NBS], cnt_c[NG], cur_s[NBS], cur_c[NG];
+    __shared__ float m[9];
+    const int b = blockIdx.x, tid = threadIdx.x, lane = tid & 31;
+    if (tid < 9) m[tid] = rotm[(size_t)b * 9 + tid];
+    for (int i = tid; i < NBS; i += blockDim.x) cnt_s[i] = 0;
+    for (int i = tid; i < NG; i += blockDim.x) cnt_c[i] = 0;
+    __syncthreads();
+    for (int l = tid; l < L.na; l += blockDim.x) {
+        const float4 a = __ldg(&L.atom[l]);
+        const float xr = rot_x(m, a.x, a.y, a.z);
+        const int sb = box_origin(xr, G.gw, G.ng) + kReach;
+        if (sb >= 0 && sb < NBS) atomicAdd(&cnt_s[sb], 1);
+        atomicAdd(&cnt_c[charge_cell(xr, G.pad, G.gw, G.ng)], 1);
+    }
+    __syncthreads();
+    int *ss = sstart + (size_t)b * (NBS + 1);
+    int *cs = cstart + (size_t)b * (NG + 1);
+    if (tid == 0) {
+        int acc = 0;
+        for (int i = 0; i < NBS; ++i) {
+            ss[i] = acc;
+            cur_s[i] = acc;
+            acc += cnt_s[i];
+        }
+        ss[NBS] = acc;
+        acc = 0;
+        for (int i = 0; i < NG; ++i) {
+            cs[i] = acc;
+            cur_c[i] = acc;
+            acc += cnt_c[i];
+        }
+        cs[NG] = acc;
+    }
+    __syncthreads();
+    MarkEntry *rb = rec + (size_t)b * L.na;
+    for (int l = tid; l < L.na; l += blockDim.x) {
+        const float4 a = __ldg(&L.atom[l]);
+        const float xr = rot_x(m, a.x, a.y, a.z);
+        const int i2 = box_origin(xr, G.gw, G.ng);
+        const int sb = i2 + kReach;
+        if (sb < 0 || sb >= NBS) continue;
+        const float yr = rot_x(m + 3, a.x, a.y, a.z);
+        const float zr = rot_x(m + 6, a.x, a.y, a.z);
+        const float2 r2 = __ldg(&L.rad2[l]);
+        const int pos = atomicAdd(&cur_s[sb], 1);
+        rb[pos].pos = make_float4(xr, yr, zr, r2.x);
+        rb[pos].box = make_int4(i2, box_origin(yr, G.gw, G.ng), box_origin(zr, G.gw, G.ng), __float_as_int(r2.y));
+    }
+    // charge entries in atom order: warp 0 walks the atoms 32 at a time
+    if (tid < 32) {
+        int2 *qb = cq + (size_t)b * L.na;
+        for (int base = 0; base < L.na; base += 32) {
+            const int l = base + lane;
+            int ie = -1, key = 0;
+            float q = 0.f;
+            if (l < L.na) {
+                const float4 a = __ldg(&L.atom[l]);
+                ie = charge_cell(rot_x(m, a.x, a.y, a.z), G.pad, G.gw, G.ng);
+                const int je = charge_cell(rot_x(m + 3, a.x, a.y, a.z), G.pad, G.gw, G.ng);
+                const int ke = charge_cell(rot_x(m + 6, a.x, a.y, a.z), G.pad, G.gw, G.ng);
+                key = je * G.ng + ke;
                 q = a.w;
             }
-        }
-        const uint32_t bal = __ballot_sync(0xffffffffu, in);
-        if (lane == 0) cs.wsum[warp] = __popc(bal);
-        __syncthreads();
-        int off = 0, total = 0;
-        for (int w = 0; w < nwarp; ++w) {
-            const int c = cs.wsum[w];
-            if (w < warp) off += c;
-            total += c;
-        }
-        if (in) {
-            const int pos = off + __popc(bal & ((1u << lane) - 1u));
-            cs.key[pos] = key;
-            cs.q[pos] = q;
-        }
-        __syncthreads();
-        if ((int)threadIdx.x < total) {
-            const int i = threadIdx.x;
-            const int ki = cs.key[i];
-            bool leader = true;
-            for (int j = 0; j < i && leader; ++j) leader = (cs.key[j] != ki);
-            if (leader) {
-                float &c = cell(ki / G.ng, ki % G.ng);
-                float acc = c;
-                for (int j = i; j < total; ++j)
-                    if (cs.key[j] == ki) acc = __fadd_rn(acc, cs.q[j]);
-                c = acc;
+            const uint32_t grp = __match_any_sync(0xffffffffu, ie);
+            int pos = 0;
+            if (ie >= 0) pos = cur_c[ie] + __popc(grp & ((1u << lane) - 1u));
+            __syncwarp();
+            if (ie >= 0) {
+                qb[pos] = make_int2(key, __float_as_int(q));
+                if (lane == 31 - __clz(grp)) cur_c[ie] += __popc(grp);
             }
+            __syncwarp();
         }
-        __syncthreads();
     }
 }
 
@@ -265,56 +279,58 @@ __device__ void vox_charges(ChargeScratch &cs, const LigandView &L, const GridVi
 //    swollen-surface scrape and the surface fill (src/ligand.cpp:20-198),
 //    stored as two bit planes: vbits[b][p][0] = "value delta",
 //    vbits[b][p][1] = "value 1.0";
-//  * imaginary part: the per-cell charge sums in ascending atom order
+//  * imaginary part: per-cell charge sums in ascending atom order from 0.0
 //    (src/ligand.cpp:200-239), stored as a compact list of the plane's charged
 //    cells qlist[b][p][e] = (q * NG + s, sum as bits), qcount[b][p] entries.
 constexpr int kNT0 = 256;
 
 template <int NG>
 __global__ void __launch_bounds__(kNT0)
-    k_vox_bits(LigandView L, GridView G, const float *__restrict__ rotm, uint32_t *__restrict__ vbits,
+    k_vox_bits(LigandView L, GridView G, const MarkEntry *__restrict__ rec, const int *__restrict__ sstart,
+               const int2 *__restrict__ cq, const int *__restrict__ cstart, uint32_t *__restrict__ vbits,
                int2 *__restrict__ qlist, int *__restrict__ qcount) {
     constexpr int W = VoxShared<NG>::W;
+    constexpr int NBS = NG + 2 * kReach;
     __shared__ VoxShared<NG> vs;
-    __shared__ MarkEntry list[kNT0];
     __shared__ uint32_t ob[2][NG * W];
-    __shared__ float qplane[NG * NG];
-    __shared__ uint32_t touched[NG * W];
-    __shared__ ChargeScratch cs;
-    __shared__ float m[9];
+    __shared__ int first[NG * NG];
     __shared__ int count;
     const int p = blockIdx.x, b = blockIdx.y, tid = threadIdx.x;
-    if (tid < 9) m[tid] = rotm[(size_t)b * 9 + tid];
     for (int w = tid; w < 5 * NG * W; w += blockDim.x) (&vs.core[0][0])[w] = 0u;
     for (int w = tid; w < 3 * NG * W; w += blockDim.x) (&vs.surf[0][0])[w] = 0u;
     for (int w = tid; w < 2 * NG * W; w += blockDim.x) (&ob[0][0])[w] = 0u;
-    for (int w = tid; w < NG * W; w += blockDim.x) touched[w] = 0u;
-    for (int c = tid; c < NG * NG; c += blockDim.x) qplane[c] = 0.f;
+    for (int c = tid; c < NG * NG; c += blockDim.x) first[c] = 0x7fffffff;
+    if (tid == 0) count = 0;
     __syncthreads();
     const bool gd = (L.delta != 1.0f);
-    vox_mark<NG>(vs, list, &count, L, G, m, p, gd);
+    const int reach = gd ? 4 : 3;
+    const int *ss = sstart + (size_t)b * (NBS + 1);
+    const int lo = ss[max(p - reach + kReach, 0)], hi = ss[min(p + reach + kReach + 1, NBS)];
+    vox_mark<NG>(vs, rec + (size_t)b * L.na, lo, hi, G, p, gd);
     for (int c = tid; c < NG * NG; c += blockDim.x) {
         const int q = c / NG, s2 = c % NG;
         const int code = vox_code<NG>(vs, p, q, s2, NG, gd);
         if (code) atomicOr(&ob[2 - code][q * W + (s2 >> 5)], 1u << (s2 & 31));
     }
-    vox_charges(cs, L, G, m, p, [&](int q, int s2) -> float & {
-        atomicOr(&touched[q * W + (s2 >> 5)], 1u << (s2 & 31));
-        return qplane[q * NG + s2];
-    });
-    // vox_charges ends with a barrier
-    uint32_t *dst = vbits + ((size_t)b * NG + p) * 2 * NG * W;
-    for (int w = tid; w < 2 * NG * W; w += blockDim.x) dst[w] = (&ob[0][0])[w];
-    if (tid == 0) count = 0;
+    // charges of this plane, in atom order: the first entry of each cell sums
+    // that cell's entries in order
+    const int c0 = cstart[(size_t)b * (NG + 1) + p], c1 = cstart[(size_t)b * (NG + 1) + p + 1];
+    const int2 *qb = cq + (size_t)b * L.na;
+    for (int e = c0 + tid; e < c1; e += blockDim.x) atomicMin(&first[qb[e].x], e);
     __syncthreads();
     int2 *ql = qlist + ((size_t)b * NG + p) * NG * NG;
-    for (int c = tid; c < NG * NG; c += blockDim.x) {
-        const int q = c / NG, s2 = c % NG;
-        if ((touched[q * W + (s2 >> 5)] >> (s2 & 31)) & 1u) {
-            const int e = atomicAdd(&count, 1);
-            ql[e] = make_int2(c, __float_as_int(qplane[c]));
+    for (int e = c0 + tid; e < c1; e += blockDim.x) {
+        const int key = qb[e].x;
+        if (first[key] != e) continue;
+        float acc = 0.f;
+        for (int f = e; f < c1; ++f) {
+            const int2 v = qb[f];
+            if (v.x == key) acc = __fadd_rn(acc, __int_as_float(v.y));
         }
+        ql[atomicAdd(&count, 1)] = make_int2(key, __float_as_int(acc));
     }
+    uint32_t *dst = vbits + ((size_t)b * NG + p) * 2 * NG * W;
+    for (int w = tid; w < 2 * NG * W; w += blockDim.x) dst[w] = (&ob[0][0])[w];
     __syncthreads();
     if (tid == 0) qcount[(size_t)b * NG + p] = count;
 }
@@ -674,7 +690,8 @@ struct TopList {
 // the N/2-point inverse FFT of Z gives s[2m] + i s[2m+1].  The scores feed a
 // per-thread top-T list directly (no score store), then a block merge writes
 // this plane's candidates cand[(b*N + x)*t + out0 + j] for j < nsel.
-// key = raw score when t == 1, raw / nf3 otherwise (src/fft_process.cpp:415, :437).
+// Keys are raw scores: ordering by raw equals ordering by raw / nf3 (a
+// positive constant), so the merge kernel divides only the winners.
 template <int N, int T>
 __global__ void __launch_bounds__(kNT, T <= 4 ? 3 : 2)
     k_plane_c2r(GridView G, const float2 *__restrict__ Gh, int t, float nf3f, int out0, int nsel,
@@ -803,10 +820,8 @@ __global__ void __launch_bounds__(kNT, T <= 4 ? 3 : 2)
             constexpr int k2 = decltype(k2_)::value;
             const int m2 = u + Q1 * k2;
             const float se = o[k2].x, so = o[k2].y;
-            const float ke = (t == 1) ? se : __fdiv_rn(se, nf3f);
-            const float ko = (t == 1) ? so : __fdiv_rn(so, nf3f);
-            top.insert(ke, base + (2 * m2) * N + z, floor);
-            top.insert(ko, base + (2 * m2 + 1) * N + z, floor);
+            top.insert(se, base + (2 * m2) * N + z, floor);
+            top.insert(so, base + (2 * m2 + 1) * N + z, floor);
         });
     }
     // block merge: nsel rounds over the per-thread heads
@@ -858,11 +873,10 @@ static __global__ void k_merge(const Cand *__restrict__ cand, int nplanes, int t
                 }
             } else {
                 // insertion below the -99999 sentinel never happens (:408-431)
-                if (idx < 0 || !(prev.key > -99999.0f)) {
+                score = idx < 0 ? -99999.0f : __fdiv_rn(prev.key, nf3f);
+                if (!(score > -99999.0f)) {
                     score = -99999.0f;
                     idx = 0;
-                } else {
-                    score = prev.key;
                 }
             }
             r.score = score;

@@ -6,6 +6,9 @@
 //   - one context per device, explicit stream, no cudaDeviceSynchronize inside
 //     the pipeline; a call returns after its own copies complete;
 //   - no cuFFT: every transform is the project's fused FFT (dock_kernels.cuh);
+//   - the batched form is one captured CUDA graph over the whole rotation
+//     range, its launch groups alternating between two work sets on two
+//     capture streams so that consecutive groups overlap on the GPU;
 //   - errors are returned as status codes with a message, never exit().
 #include <cuda_runtime.h>
 
@@ -23,10 +26,64 @@
 
 using namespace mdb;
 
+namespace {
+
+// Per-launch intermediates for `cap` rotations of one launch group.
+struct WorkSet {
+    float2 *A = nullptr;        // [cap][N/2][N][N]    spectrum planes (K1 -> K2)
+    float2 *G = nullptr;        // [cap][N][N/2][N]    Hermitian half (K2 -> K3)
+    Cand *cand = nullptr;       // [cap][N][t]         per-plane candidates (K3 -> K4)
+    uint32_t *vbits = nullptr;  // [cap][N/2][2][N/2 * words per row] voxel classes (K0 -> K1)
+    int2 *qlist = nullptr;      // [cap][N/2][(N/2)^2] charged cells per voxel plane (K0 -> K1)
+    int *qcount = nullptr;      // [cap][N/2]
+    MarkEntry *srec = nullptr;  // [cap][na]           atom records bucketed by plane (prep -> K0)
+    int *sstart = nullptr;      // [cap][N/2 + 2 kReach + 1]
+    int2 *cq = nullptr;         // [cap][na]           charge entries bucketed by plane, atom order
+    int *cstart = nullptr;      // [cap][N/2 + 1]
+
+    void release() {
+        cudaFree(A);
+        cudaFree(G);
+        cudaFree(cand);
+        cudaFree(vbits);
+        cudaFree(qlist);
+        cudaFree(qcount);
+        cudaFree(srec);
+        cudaFree(sstart);
+        cudaFree(cq);
+        cudaFree(cstart);
+        *this = WorkSet();
+    }
+    cudaError_t allocate(size_t cap, size_t N, size_t t, size_t na) {
+        const size_t NG = N / 2;
+        cudaError_t e = cudaSuccess;
+        auto get = [&](auto **p, size_t bytes) {
+            if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void **>(p), bytes);
+        };
+        get(&A, sizeof(float2) * cap * NG * N * N);
+        get(&G, sizeof(float2) * cap * N * (N / 2) * N);
+        get(&cand, sizeof(Cand) * cap * N * t);
+        get(&vbits, sizeof(uint32_t) * cap * NG * 2 * NG * ((NG + 31) / 32));
+        get(&qlist, sizeof(int2) * cap * NG * NG * NG);
+        get(&qcount, sizeof(int) * cap * NG);
+        get(&srec, sizeof(MarkEntry) * cap * na);
+        get(&sstart, sizeof(int) * cap * (NG + 2 * kReach + 1));
+        get(&cq, sizeof(int2) * cap * na);
+        get(&cstart, sizeof(int) * cap * (NG + 1));
+        return e;
+    }
+};
+
+constexpr int kLanes = 2;
+
+}  // namespace
+
 struct md_ctx {
     int device = 0;
     cudaStream_t own = nullptr;
     cudaStream_t stream = nullptr;
+    cudaStream_t side = nullptr;     // second capture stream of the batched form
+    cudaEvent_t fork = nullptr, join = nullptr;
     std::string err;
     // grid
     int N = 0, ng = 0;
@@ -37,21 +94,15 @@ struct md_ctx {
     float2 *d_Rh = nullptr;
     bool have_receptor = false;
     // ligand
-    int na = 0;
+    int na = 0, na_cap = 0;
     float delta = 1.0f;
     float4 *d_atom = nullptr;
     float2 *d_rad2 = nullptr;
     bool have_ligand = false;
-    // per-launch work buffers, sized for `cap` rotations
+    // work sets (lane 0 serves every form; lane 1 the batched graph)
     int batch = 1;
-    int cap = 0;
-    int cap_t = 0;
-    float2 *d_A = nullptr;   // [cap][ng][N][N]
-    float2 *d_G = nullptr;   // [cap][N][N/2][N] (Hermitian half of the x-inverted product)
-    Cand *d_cand = nullptr;  // [cap][N][t]
-    uint32_t *d_vbits = nullptr;   // [cap][N/2][2][N/2 * words per row] voxel class bit planes
-    int2 *d_qlist = nullptr;       // [cap][N/2][(N/2)^2] charged cells of each voxel plane
-    int *d_qcount = nullptr;       // [cap][N/2]
+    int cap = 0, cap_t = 0, cap_na = 0;
+    WorkSet ws[kLanes];
     // staging for host-buffer calls
     float *d_rot = nullptr;
     size_t rot_cap = 0;
@@ -109,16 +160,26 @@ struct Sized {
         GridView G{c->ng, c->gw, 0.f, c->d_gc, c->d_tw};
         LigandView L{0, nullptr, nullptr, 1.f};
         k_plane_fwd<N, 1><<<dim3(NG, 1), kNT, smem_fwd(), c->stream>>>(L, G, nullptr, nullptr, nullptr, d_r, d_i,
-                                                                        c->d_A, nullptr, nullptr);
-        k_xline_rec<N><<<dim3(N * TILES, 1), kNT, 0, c->stream>>>(G, c->d_A, c->d_Rh);
+                                                                        c->ws[0].A, nullptr, nullptr);
+        k_xline_rec<N><<<dim3(N * TILES, 1), kNT, 0, c->stream>>>(G, c->ws[0].A, c->d_Rh);
+    }
+
+    // Voxelizer of one launch group (atom prep + K0).
+    static void voxelize(md_ctx *c, const WorkSet &w, const float *d_rot9, int nb, cudaStream_t s) {
+        GridView G{c->ng, c->gw, (float)(c->ng * c->gw) / 2, c->d_gc, c->d_tw};
+        LigandView L{c->na, c->d_atom, c->d_rad2, c->delta};
+        k_atom_prep<NG><<<nb, kNTP, 0, s>>>(L, G, d_rot9, w.srec, w.sstart, w.cq, w.cstart);
+        k_vox_bits<NG><<<dim3(NG, nb), kNT0, 0, s>>>(L, G, w.srec, w.sstart, w.cq, w.cstart, w.vbits, w.qlist,
+                                                    w.qcount);
     }
 
     static void voxels(md_ctx *c, const float *d_rot9, float *d_vr, float *d_vi) {
         GridView G{c->ng, c->gw, (float)(c->ng * c->gw) / 2, c->d_gc, c->d_tw};
         LigandView L{c->na, c->d_atom, c->d_rad2, c->delta};
-        k_vox_bits<NG><<<dim3(NG, 1), kNT0, 0, c->stream>>>(L, G, d_rot9, c->d_vbits, c->d_qlist, c->d_qcount);
-        k_plane_fwd<N, 2><<<dim3(NG, 1), kNT, smem_fwd(), c->stream>>>(L, G, c->d_vbits, c->d_qlist, c->d_qcount,
-                                                                        nullptr, nullptr, nullptr, d_vr, d_vi);
+        const WorkSet &w = c->ws[0];
+        voxelize(c, w, d_rot9, 1, c->stream);
+        k_plane_fwd<N, 2><<<dim3(NG, 1), kNT, smem_fwd(), c->stream>>>(L, G, w.vbits, w.qlist, w.qcount, nullptr,
+                                                                        nullptr, nullptr, d_vr, d_vi);
     }
 
     // The plane top-t kernel in passes of T candidates (T = 1, 4 or 16).
@@ -135,24 +196,25 @@ struct Sized {
         }
     }
 
-    // One launch group: nb rotations whose matrices start at d_rot9.  With
-    // `ev` set, an event is recorded after each of the five stages.
-    static void dock(md_ctx *c, const float *d_rot9, int nb, int rot0, int t, DevPose *d_pose,
-                     cudaEvent_t *ev = nullptr) {
+    // One launch group: nb rotations whose matrices start at d_rot9, on work
+    // set w and stream s.  With `ev` set, an event is recorded after each of
+    // the five stages.
+    static void dock(md_ctx *c, const WorkSet &w, cudaStream_t s, const float *d_rot9, int nb, int rot0, int t,
+                     DevPose *d_pose, cudaEvent_t *ev) {
         GridView G{c->ng, c->gw, (float)(c->ng * c->gw) / 2, c->d_gc, c->d_tw};
         LigandView L{c->na, c->d_atom, c->d_rad2, c->delta};
         const float nf3f = (float)((long long)N * N * N);
-        k_vox_bits<NG><<<dim3(NG, nb), kNT0, 0, c->stream>>>(L, G, d_rot9, c->d_vbits, c->d_qlist, c->d_qcount);
-        if (ev) cudaEventRecord(ev[1], c->stream);
-        k_plane_fwd<N, 0><<<dim3(NG, nb), kNT, smem_fwd(), c->stream>>>(L, G, c->d_vbits, c->d_qlist, c->d_qcount,
-                                                                         nullptr, nullptr, c->d_A, nullptr, nullptr);
-        if (ev) cudaEventRecord(ev[2], c->stream);
-        k_xline_herm<N><<<dim3(NH * TILES, nb), kNT, smem_xline(), c->stream>>>(G, c->d_A, c->d_Rh, c->d_G);
-        if (ev) cudaEventRecord(ev[3], c->stream);
-        plane_topt(c->stream, G, c->d_G, nb, t, nf3f, c->d_cand);
-        if (ev) cudaEventRecord(ev[4], c->stream);
-        k_merge<<<nb, 256, 0, c->stream>>>(c->d_cand, N, t, N, nf3f, rot0, d_pose);
-        if (ev) cudaEventRecord(ev[5], c->stream);
+        voxelize(c, w, d_rot9, nb, s);
+        if (ev) cudaEventRecord(ev[1], s);
+        k_plane_fwd<N, 0><<<dim3(NG, nb), kNT, smem_fwd(), s>>>(L, G, w.vbits, w.qlist, w.qcount, nullptr, nullptr,
+                                                                w.A, nullptr, nullptr);
+        if (ev) cudaEventRecord(ev[2], s);
+        k_xline_herm<N><<<dim3(NH * TILES, nb), kNT, smem_xline(), s>>>(G, w.A, c->d_Rh, w.G);
+        if (ev) cudaEventRecord(ev[3], s);
+        plane_topt(s, G, w.G, nb, t, nf3f, w.cand);
+        if (ev) cudaEventRecord(ev[4], s);
+        k_merge<<<nb, 256, 0, s>>>(w.cand, N, t, N, nf3f, rot0, d_pose);
+        if (ev) cudaEventRecord(ev[5], s);
     }
 };
 
@@ -197,10 +259,11 @@ void launch_voxels(md_ctx *c, const float *rot, float *vr, float *vi) {
     }
 }
 
-void launch_dock(md_ctx *c, const float *rot, int nb, int rot0, int t, DevPose *pose, cudaEvent_t *ev = nullptr) {
+void launch_dock(md_ctx *c, int lane, cudaStream_t s, const float *rot, int nb, int rot0, int t, DevPose *pose,
+                 cudaEvent_t *ev = nullptr) {
     switch (c->N) {
 #define X(n) \
-    case n: Sized<n>::dock(c, rot, nb, rot0, t, pose, ev); break;
+    case n: Sized<n>::dock(c, c->ws[lane], s, rot, nb, rot0, t, pose, ev); break;
         MDB_SIZES(X)
 #undef X
     }
@@ -211,33 +274,23 @@ void free_graphs(md_ctx *c) {
     c->graphs.clear();
 }
 
+void release_work(md_ctx *c) {
+    free_graphs(c);
+    for (auto &w : c->ws) w.release();
+    c->cap = c->cap_t = c->cap_na = 0;
+}
+
+// Work sets for launch groups of `cap` rotations with t poses each.
 int ensure_work(md_ctx *ctx, int cap, int t) {
-    if (cap <= ctx->cap && t <= ctx->cap_t) return MD_OK;
-    free_graphs(ctx);
-    cudaFree(ctx->d_A);
-    cudaFree(ctx->d_G);
-    cudaFree(ctx->d_cand);
-    cudaFree(ctx->d_vbits);
-    cudaFree(ctx->d_qlist);
-    cudaFree(ctx->d_qcount);
-    ctx->d_A = nullptr;
-    ctx->d_G = nullptr;
-    ctx->d_cand = nullptr;
-    ctx->d_vbits = nullptr;
-    ctx->d_qlist = nullptr;
-    ctx->d_qcount = nullptr;
-    ctx->cap = ctx->cap_t = 0;
-    const size_t N = ctx->N, NG = ctx->ng;
-    cap = std::max(cap, 1);
-    t = std::max(t, 1);
-    MD_CUDA(cudaMalloc(&ctx->d_A, sizeof(float2) * cap * NG * N * N));
-    MD_CUDA(cudaMalloc(&ctx->d_G, sizeof(float2) * cap * N * (N / 2) * N));
-    MD_CUDA(cudaMalloc(&ctx->d_cand, sizeof(Cand) * cap * N * t));
-    MD_CUDA(cudaMalloc(&ctx->d_vbits, sizeof(uint32_t) * cap * NG * 2 * NG * ((NG + 31) / 32)));
-    MD_CUDA(cudaMalloc(&ctx->d_qlist, sizeof(int2) * cap * NG * NG * NG));
-    MD_CUDA(cudaMalloc(&ctx->d_qcount, sizeof(int) * cap * NG));
+    if (cap <= ctx->cap && t <= ctx->cap_t && ctx->na <= ctx->cap_na) return MD_OK;
+    cap = std::max({cap, ctx->cap, 1});
+    t = std::max({t, ctx->cap_t, 1});
+    const int na = std::max({ctx->na, ctx->cap_na, 1});
+    release_work(ctx);
+    for (auto &w : ctx->ws) MD_CUDA(w.allocate(cap, ctx->N, t, na));
     ctx->cap = cap;
     ctx->cap_t = t;
+    ctx->cap_na = na;
     return MD_OK;
 }
 
@@ -264,20 +317,29 @@ int run_dock(md_ctx *ctx, const float *d_rot, int first_rot, int n_rot, int t, D
     if (rc) return rc;
     if (B == 1) {
         // plain form: one rotation per fused pipeline, launched back to back
-        for (int r = 0; r < n_rot; ++r) launch_dock(ctx, d_rot + 9 * (size_t)r, 1, first_rot + r, t, d_pose + (size_t)r * t);
+        for (int r = 0; r < n_rot; ++r)
+            launch_dock(ctx, 0, ctx->stream, d_rot + 9 * (size_t)r, 1, first_rot + r, t, d_pose + (size_t)r * t);
         MD_CUDA(cudaGetLastError());
         return MD_OK;
     }
-    // batched form: the whole rotation loop as one captured CUDA graph
+    // batched form: the whole rotation loop as one captured CUDA graph; launch
+    // groups alternate between the two work sets and the two capture streams
     auto key = std::make_tuple(first_rot, n_rot, t, B, d_rot, d_pose);
     auto it = ctx->graphs.find(key);
     if (it == ctx->graphs.end()) {
         cudaGraph_t g;
         MD_CUDA(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
-        for (int r = 0; r < n_rot; r += B) {
+        cudaEventRecord(ctx->fork, ctx->stream);
+        cudaStreamWaitEvent(ctx->side, ctx->fork, 0);
+        int group = 0;
+        for (int r = 0; r < n_rot; r += B, ++group) {
             const int nb = std::min(B, n_rot - r);
-            launch_dock(ctx, d_rot + 9 * (size_t)r, nb, first_rot + r, t, d_pose + (size_t)r * t);
+            const int lane = group % kLanes;
+            launch_dock(ctx, lane, lane ? ctx->side : ctx->stream, d_rot + 9 * (size_t)r, nb, first_rot + r, t,
+                        d_pose + (size_t)r * t);
         }
+        cudaEventRecord(ctx->join, ctx->side);
+        cudaStreamWaitEvent(ctx->stream, ctx->join, 0);
         cudaError_t ce = cudaStreamEndCapture(ctx->stream, &g);
         if (ce != cudaSuccess) {
             ctx->err = std::string("graph capture: ") + cudaGetErrorString(ce);
@@ -311,7 +373,10 @@ int md_ctx_create(int device, md_ctx **out) {
     md_ctx *ctx = new md_ctx;
     ctx->device = device;
     if (cudaSetDevice(device) != cudaSuccess ||
-        cudaStreamCreateWithFlags(&ctx->own, cudaStreamNonBlocking) != cudaSuccess) {
+        cudaStreamCreateWithFlags(&ctx->own, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&ctx->side, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&ctx->fork, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&ctx->join, cudaEventDisableTiming) != cudaSuccess) {
         delete ctx;
         return MD_ERR_CUDA;
     }
@@ -324,20 +389,18 @@ void md_ctx_destroy(md_ctx *ctx) {
     if (!ctx) return;
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
-    free_graphs(ctx);
+    cudaStreamSynchronize(ctx->side);
+    release_work(ctx);
     cudaFree(ctx->d_gc);
     cudaFree(ctx->d_tw);
     cudaFree(ctx->d_Rh);
     cudaFree(ctx->d_atom);
     cudaFree(ctx->d_rad2);
-    cudaFree(ctx->d_A);
-    cudaFree(ctx->d_G);
-    cudaFree(ctx->d_cand);
-    cudaFree(ctx->d_vbits);
-    cudaFree(ctx->d_qlist);
-    cudaFree(ctx->d_qcount);
     cudaFree(ctx->d_rot);
     cudaFree(ctx->d_pose);
+    if (ctx->fork) cudaEventDestroy(ctx->fork);
+    if (ctx->join) cudaEventDestroy(ctx->join);
+    if (ctx->side) cudaStreamDestroy(ctx->side);
     if (ctx->own) cudaStreamDestroy(ctx->own);
     delete ctx;
 }
@@ -360,25 +423,13 @@ int md_set_grid(md_ctx *ctx, int nf1, float grid_width, const float *grid_coord)
     MD_CUDA(cudaSetDevice(ctx->device));
     MD_CUDA(set_attrs(nf1));
     if (ctx->N != nf1) {
-        free_graphs(ctx);
+        release_work(ctx);
         cudaFree(ctx->d_gc);
         cudaFree(ctx->d_tw);
         cudaFree(ctx->d_Rh);
-        cudaFree(ctx->d_A);
-        cudaFree(ctx->d_G);
-        cudaFree(ctx->d_cand);
-        cudaFree(ctx->d_vbits);
-        cudaFree(ctx->d_qlist);
-        cudaFree(ctx->d_qcount);
-        ctx->d_vbits = nullptr;
-        ctx->d_qlist = nullptr;
-        ctx->d_qcount = nullptr;
         ctx->d_gc = nullptr;
         ctx->d_tw = nullptr;
         ctx->d_Rh = nullptr;
-        ctx->d_A = ctx->d_G = nullptr;
-        ctx->d_cand = nullptr;
-        ctx->cap = ctx->cap_t = 0;
         ctx->have_receptor = false;
         const size_t N = nf1;
         MD_CUDA(cudaMalloc(&ctx->d_gc, sizeof(float) * N / 2));
@@ -394,6 +445,7 @@ int md_set_grid(md_ctx *ctx, int nf1, float grid_width, const float *grid_coord)
         ctx->N = nf1;
         ctx->ng = nf1 / 2;
     }
+    if (ctx->gw != grid_width) free_graphs(ctx);   // the grid width is a kernel argument
     ctx->gw = grid_width;
     MD_CUDA(cudaMemcpyAsync(ctx->d_gc, grid_coord, sizeof(float) * ctx->ng, cudaMemcpyHostToDevice, ctx->stream));
     MD_CUDA(cudaStreamSynchronize(ctx->stream));
@@ -465,19 +517,26 @@ int md_ligand_data(md_ctx *ctx, int na, const float *xyz, const float *radius, c
         const float r = radius[l];
         rad[l] = make_float2(r * r * 1.5f, r * r * 1.0f);
     }
-    cudaFree(ctx->d_atom);
-    cudaFree(ctx->d_rad2);
-    ctx->d_atom = nullptr;
-    ctx->d_rad2 = nullptr;
-    MD_CUDA(cudaMalloc(&ctx->d_atom, sizeof(float4) * na));
-    MD_CUDA(cudaMalloc(&ctx->d_rad2, sizeof(float2) * na));
+    if (na > ctx->na_cap) {
+        free_graphs(ctx);
+        cudaFree(ctx->d_atom);
+        cudaFree(ctx->d_rad2);
+        ctx->d_atom = nullptr;
+        ctx->d_rad2 = nullptr;
+        ctx->na_cap = 0;
+        MD_CUDA(cudaMalloc(&ctx->d_atom, sizeof(float4) * na));
+        MD_CUDA(cudaMalloc(&ctx->d_rad2, sizeof(float2) * na));
+        ctx->na_cap = na;
+    }
+    // captured graphs hold the atom count and core value as kernel arguments;
+    // new coordinates in the same buffers keep them valid
+    if (na != ctx->na || lig_core != ctx->delta) free_graphs(ctx);
     MD_CUDA(cudaMemcpyAsync(ctx->d_atom, atom.data(), sizeof(float4) * na, cudaMemcpyHostToDevice, ctx->stream));
     MD_CUDA(cudaMemcpyAsync(ctx->d_rad2, rad.data(), sizeof(float2) * na, cudaMemcpyHostToDevice, ctx->stream));
     MD_CUDA(cudaStreamSynchronize(ctx->stream));
     ctx->na = na;
     ctx->delta = lig_core;
     ctx->have_ligand = true;
-    free_graphs(ctx);
     return MD_OK;
 }
 
@@ -538,12 +597,15 @@ int md_dock_profile(md_ctx *ctx, const float *d_rot, int first_rot, int n_rot, i
     for (auto &e : ev) MD_CUDA(cudaEventCreate(&e));
     double acc[5] = {0, 0, 0, 0, 0};
     int nl = 0;
+    // atom prep, voxelizer, forward planes, x lines, one top-t pass per T poses, merge
+    const int T = t == 1 ? 1 : (t <= 4 ? 4 : 16);
+    const int per_group = 5 + (t + T - 1) / T;
     for (int r = 0; r < n_rot; r += B) {
         const int nb = std::min(B, n_rot - r);
         MD_CUDA(cudaEventRecord(ev[0], ctx->stream));
-        launch_dock(ctx, d_rot + 9 * (size_t)r, nb, first_rot + r, t,
+        launch_dock(ctx, 0, ctx->stream, d_rot + 9 * (size_t)r, nb, first_rot + r, t,
                     reinterpret_cast<DevPose *>(d_out) + (size_t)r * t, ev);
-        nl += 5;
+        nl += per_group;
         MD_CUDA(cudaEventSynchronize(ev[5]));
         for (int k = 0; k < 5; ++k) {
             float ms = 0.f;
@@ -565,6 +627,8 @@ int md_ligand_voxels(md_ctx *ctx, const float *rotmat9, float *grid_r, float *gr
         return MD_ERR_STATE;
     }
     MD_CUDA(cudaSetDevice(ctx->device));
+    int rc = ensure_work(ctx, std::max(1, ctx->batch), 1);
+    if (rc) return rc;
     const size_t ng3 = (size_t)ctx->ng * ctx->ng * ctx->ng;
     float *d = nullptr;
     MD_CUDA(cudaMalloc(&d, sizeof(float) * (ng3 * 2 + 9)));

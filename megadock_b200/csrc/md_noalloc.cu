@@ -127,13 +127,21 @@ __global__ void k_pack_ligand(int na, const float *__restrict__ xyz, const float
     rad2[l] = make_float2(__fmul_rn(__fmul_rn(r, r), 1.5f), __fmul_rn(__fmul_rn(r, r), 1.0f));
 }
 
+struct Prep {
+    MarkEntry *srec;
+    int *sstart;
+    int2 *cq;
+    int *cstart;
+};
+
 template <int N>
 void run_rotation(cudaStream_t s, const LigandView &L, const GridView &G, const float *rot9, const float2 *Rh,
-                  uint32_t *vbits, int2 *qlist, int *qcount, float2 *A, float2 *Gsp, Cand *cand, int rot, int t,
-                  DevPose *pose) {
+                  const Prep &pr, uint32_t *vbits, int2 *qlist, int *qcount, float2 *A, float2 *Gsp, Cand *cand,
+                  int rot, int t, DevPose *pose) {
     constexpr int NG = N / 2, NH = N / 2, TILES = (N + kLT - 1) / kLT;
     const float nf3f = (float)((long long)N * N * N);
-    k_vox_bits<NG><<<dim3(NG, 1), kNT0, 0, s>>>(L, G, rot9, vbits, qlist, qcount);
+    k_atom_prep<NG><<<1, kNTP, 0, s>>>(L, G, rot9, pr.srec, pr.sstart, pr.cq, pr.cstart);
+    k_vox_bits<NG><<<dim3(NG, 1), kNT0, 0, s>>>(L, G, pr.srec, pr.sstart, pr.cq, pr.cstart, vbits, qlist, qcount);
     k_plane_fwd<N, 0><<<dim3(NG, 1), kNT, Smem<N>::fwd(), s>>>(L, G, vbits, qlist, qcount, nullptr, nullptr, A,
                                                                nullptr, nullptr);
     k_xline_herm<N><<<dim3(NH * TILES, 1), kNT, Smem<N>::xline(), s>>>(G, A, Rh, Gsp);
@@ -168,7 +176,10 @@ extern "C" int md_dock_noalloc(int nf1, float grid_width, const float *d_grid_co
     const size_t b_cand = up(sizeof(Cand) * N * t);
     const size_t b_bits = up(sizeof(uint32_t) * NG * 2 * NG * ((NG + 31) / 32));
     const size_t b_ql = up(sizeof(int2) * NG * NG * NG), b_qc = up(sizeof(int) * NG);
-    if (b_atom + b_rad + b_A + b_G + b_cand + b_bits + b_ql + b_qc > kScratchBytes) return MD_ERR_SIZE;
+    const size_t b_sr = up(sizeof(MarkEntry) * na), b_ss = up(sizeof(int) * (NG + 2 * kReach + 1));
+    const size_t b_cq = up(sizeof(int2) * na), b_cs = up(sizeof(int) * (NG + 1));
+    const size_t used = b_atom + b_rad + b_A + b_G + b_cand + b_bits + b_ql + b_qc + b_sr + b_ss + b_cq + b_cs;
+    if (used > kScratchBytes) return MD_ERR_SIZE;
     if (n_rot == 0) return MD_OK;
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return MD_ERR_CUDA;
@@ -184,6 +195,9 @@ extern "C" int md_dock_noalloc(int nf1, float grid_width, const float *d_grid_co
     uint32_t *vbits = reinterpret_cast<uint32_t *>(p + b_atom + b_rad + b_A + b_G + b_cand);
     int2 *qlist = reinterpret_cast<int2 *>(p + b_atom + b_rad + b_A + b_G + b_cand + b_bits);
     int *qcount = reinterpret_cast<int *>(p + b_atom + b_rad + b_A + b_G + b_cand + b_bits + b_ql);
+    unsigned char *q0 = p + b_atom + b_rad + b_A + b_G + b_cand + b_bits + b_ql + b_qc;
+    const Prep prep{reinterpret_cast<MarkEntry *>(q0), reinterpret_cast<int *>(q0 + b_sr),
+                    reinterpret_cast<int2 *>(q0 + b_sr + b_ss), reinterpret_cast<int *>(q0 + b_sr + b_ss + b_cq)};
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     k_pack_ligand<<<(na + 255) / 256, 256, 0, s>>>(na, d_xyz_centred, d_radius, d_charge, atom, rad2);
     GridView G{(int)NG, grid_width, (float)((int)NG * grid_width) / 2, d_grid_coord, st.twiddle + tw_offset(nf1)};
@@ -195,7 +209,7 @@ extern "C" int md_dock_noalloc(int nf1, float grid_width, const float *d_grid_co
         DevPose *pr = pose + (size_t)r * t;
         switch (nf1) {
 #define X(n) \
-    case n: run_rotation<n>(s, L, G, rot9, Rh, vbits, qlist, qcount, A, Gsp, cand, first_rot + r, t, pr); break;
+    case n: run_rotation<n>(s, L, G, rot9, Rh, prep, vbits, qlist, qcount, A, Gsp, cand, first_rot + r, t, pr); break;
             X(32) X(48) X(64) X(80) X(96) X(112) X(120) X(128)
 #undef X
         }
