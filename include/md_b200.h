@@ -87,6 +87,18 @@ int md_dock(md_ctx *ctx, const float *rotmat, int first_rot, int n_rot, int t, m
 /* Same with device-resident rotation matrices and device output buffer. */
 int md_dock_device(md_ctx *ctx, const float *d_rotmat, int first_rot, int n_rot, int t, md_pose *d_out);
 
+/* Batched form over many receptor-ligand pairs of uneven FFT sizes: the
+ * reference docks one pair per process and farms pairs out over MPI
+ * (src/mpidp.cpp:281-551); here every pair's rotations run in one captured
+ * CUDA graph on `runner`'s stream and work buffers.  pairs[p] is a context
+ * prepared for pair p (md_set_grid, md_receptor_fft, md_ligand_data, and its
+ * rotations per launch from md_set_batch) on the runner's device;
+ * d_rotmat[p] holds 9 * n_rot[p] floats and d_out[p] receives n_rot[p] * t
+ * poses (device buffers).  Rotation numbers in the poses count from 0 per
+ * pair.  Asynchronous on the runner's stream. */
+int md_dock_pairs(md_ctx *runner, md_ctx *const *pairs, int npairs, const float *const *d_rotmat, const int *n_rot,
+                  int t, md_pose *const *d_out);
+
 /* Per-stage device time of md_dock_device's launches (no graph): stage_ms[5]
  * receives the summed CUDA-event time of the voxelizer (rotation, rPSC classes
  * and ordered charge sums), the forward-plane kernel (y/z FFT), the x-line

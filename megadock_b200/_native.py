@@ -50,6 +50,8 @@ _PROTOS = {
     "md_set_batch": (C.c_int, [_VP, C.c_int]),
     "md_dock": (C.c_int, [_VP, _FP, C.c_int, C.c_int, C.c_int, _VP]),
     "md_dock_device": (C.c_int, [_VP, _VP, C.c_int, C.c_int, C.c_int, _VP]),
+    "md_dock_pairs": (C.c_int, [_VP, C.POINTER(_VP), C.c_int, C.POINTER(_VP), C.POINTER(C.c_int), C.c_int,
+                                C.POINTER(_VP)]),
     "md_ligand_voxels": (C.c_int, [_VP, _FP, _FP, _FP]),
     "md_dock_profile": (C.c_int, [_VP, _VP, C.c_int, C.c_int, C.c_int, _VP, _FP, _IP]),
     "md_dock_noalloc": (C.c_int, [C.c_int, C.c_float, _VP, _VP, C.c_int, _VP, _VP, _VP, C.c_float, _VP, C.c_int,

@@ -480,6 +480,7 @@ __global__ void __launch_bounds__(kNT)
     k_xline_herm(GridView G, const float2 *__restrict__ A, const float2 *__restrict__ Rh, float2 *__restrict__ Gh) {
     constexpr int NG = N / 2, NH = N / 2, OFF = N / 4;
     constexpr int R1 = Plan<N>::R1, R2 = Plan<N>::R2;
+    static_assert(R1 % 4 == 0, "pruned forward x pass needs R1 % 4 == 0");
     constexpr int TILES = (N + kLT - 1) / kLT;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     float2 *X0 = reinterpret_cast<float2 *>(smem_raw);   // own tile   [N][kLT]
@@ -692,8 +693,14 @@ struct TopList {
 // this plane's candidates cand[(b*N + x)*t + out0 + j] for j < nsel.
 // Keys are raw scores: ordering by raw equals ordering by raw / nf3 (a
 // positive constant), so the merge kernel divides only the winners.
+// Three CTAs per SM (<= 42 registers) where the radices are small enough.
 template <int N, int T>
-__global__ void __launch_bounds__(kNT, T <= 4 ? 3 : 2)
+constexpr int c2r_min_blocks() {
+    return (T <= 4 && Plan<N>::R1 <= 8 && Plan<N>::R2 <= 16 && Plan<N / 2>::R1 <= 8 && Plan<N / 2>::R2 <= 16) ? 3 : 2;
+}
+
+template <int N, int T>
+__global__ void __launch_bounds__(kNT, c2r_min_blocks<N, T>())
     k_plane_c2r(GridView G, const float2 *__restrict__ Gh, int t, float nf3f, int out0, int nsel,
                 Cand *__restrict__ cand) {
     constexpr int NH = N / 2;

@@ -192,7 +192,9 @@ struct Dft {
 };
 
 // ------------------------------------------------------------------ line plans
-// Supported FFT edge lengths and their split N = R1 * R2 (R1 % 4 == 0).
+// Supported FFT edge lengths and their split N = R1 * R2.  Edges that carry the
+// zero-padded ligand / receptor (N % 4 == 0) use R1 % 4 == 0 so the pruned
+// first pass works; the half edges of the complex-to-real pass need not.
 template <int N>
 struct Plan;
 #define MDB_PLAN(N_, R1_, R2_)                                  \
@@ -200,19 +202,24 @@ struct Plan;
     struct Plan<N_> {                                            \
         static constexpr int R1 = R1_;                           \
         static constexpr int R2 = R2_;                           \
-        static_assert(R1_ * R2_ == N_ && R1_ % 4 == 0, "plan");  \
+        static_assert(R1_ * R2_ == N_, "plan");                  \
     };
 MDB_PLAN(16, 4, 4)
 MDB_PLAN(24, 4, 6)
 MDB_PLAN(32, 4, 8)
+MDB_PLAN(36, 4, 9)
 MDB_PLAN(40, 8, 5)
 MDB_PLAN(48, 4, 12)
+MDB_PLAN(50, 10, 5)
+MDB_PLAN(54, 6, 9)
 MDB_PLAN(56, 8, 7)
 MDB_PLAN(60, 4, 15)
 MDB_PLAN(64, 8, 8)
 MDB_PLAN(72, 8, 9)
 MDB_PLAN(80, 8, 10)
 MDB_PLAN(96, 8, 12)
+MDB_PLAN(100, 20, 5)
+MDB_PLAN(108, 12, 9)
 MDB_PLAN(112, 8, 14)
 MDB_PLAN(120, 8, 15)
 MDB_PLAN(128, 8, 16)
@@ -225,6 +232,7 @@ MDB_PLAN(160, 16, 10)
 template <int N, int S, bool PRUNE>
 __device__ __forceinline__ void fft_phase1(float2 *b, int es, int t, const float2 *__restrict__ tw) {
     constexpr int R1 = Plan<N>::R1, R2 = Plan<N>::R2;
+    static_assert(!PRUNE || R1 % 4 == 0, "pruned first pass needs R1 % 4 == 0");
     float2 v[R1];
     static_for<0, R1>([&](auto m_) {
         constexpr int m = decltype(m_)::value;

@@ -54,22 +54,22 @@ struct WorkSet {
         cudaFree(cstart);
         *this = WorkSet();
     }
-    cudaError_t allocate(size_t cap, size_t N, size_t t, size_t na) {
+    // Bytes of each buffer for launch groups of `cap` rotations.
+    struct Sizes {
+        size_t b[10];
+    };
+    static Sizes need(size_t cap, size_t N, size_t t, size_t na) {
         const size_t NG = N / 2;
+        return Sizes{{sizeof(float2) * cap * NG * N * N, sizeof(float2) * cap * N * (N / 2) * N,
+                      sizeof(Cand) * cap * N * t, sizeof(uint32_t) * cap * NG * 2 * NG * ((NG + 31) / 32),
+                      sizeof(int2) * cap * NG * NG * NG, sizeof(int) * cap * NG, sizeof(MarkEntry) * cap * na,
+                      sizeof(int) * cap * (NG + 2 * kReach + 1), sizeof(int2) * cap * na, sizeof(int) * cap * (NG + 1)}};
+    }
+    cudaError_t allocate(const Sizes &z) {
         cudaError_t e = cudaSuccess;
-        auto get = [&](auto **p, size_t bytes) {
-            if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void **>(p), bytes);
-        };
-        get(&A, sizeof(float2) * cap * NG * N * N);
-        get(&G, sizeof(float2) * cap * N * (N / 2) * N);
-        get(&cand, sizeof(Cand) * cap * N * t);
-        get(&vbits, sizeof(uint32_t) * cap * NG * 2 * NG * ((NG + 31) / 32));
-        get(&qlist, sizeof(int2) * cap * NG * NG * NG);
-        get(&qcount, sizeof(int) * cap * NG);
-        get(&srec, sizeof(MarkEntry) * cap * na);
-        get(&sstart, sizeof(int) * cap * (NG + 2 * kReach + 1));
-        get(&cq, sizeof(int2) * cap * na);
-        get(&cstart, sizeof(int) * cap * (NG + 1));
+        void **slot[10] = {(void **)&A, (void **)&G, (void **)&cand, (void **)&vbits, (void **)&qlist,
+                           (void **)&qcount, (void **)&srec, (void **)&sstart, (void **)&cq, (void **)&cstart};
+        for (int k = 0; k < 10 && e == cudaSuccess; ++k) e = cudaMalloc(slot[k], z.b[k]);
         return e;
     }
 };
@@ -102,6 +102,7 @@ struct md_ctx {
     // work sets (lane 0 serves every form; lane 1 the batched graph)
     int batch = 1;
     int cap = 0, cap_t = 0, cap_na = 0;
+    WorkSet::Sizes have{};           // bytes held by each work-set buffer
     WorkSet ws[kLanes];
     // staging for host-buffer calls
     float *d_rot = nullptr;
@@ -110,6 +111,8 @@ struct md_ctx {
     size_t pose_cap = 0;
     // captured graphs of the batched form: (first_rot, n_rot, t, batch, rot ptr, pose ptr)
     std::map<std::tuple<int, int, int, int, const float *, DevPose *>, cudaGraphExec_t> graphs;
+    // captured graphs of md_dock_pairs, keyed by every argument
+    std::map<std::vector<uintptr_t>, cudaGraphExec_t> pair_graphs;
 };
 
 static_assert(sizeof(md_pose) == sizeof(DevPose), "pose layout");
@@ -218,7 +221,7 @@ struct Sized {
     }
 };
 
-#define MDB_SIZES(X) X(32) X(48) X(64) X(80) X(96) X(112) X(120) X(128) X(144) X(160)
+#define MDB_SIZES(X) X(32) X(48) X(64) X(72) X(80) X(96) X(100) X(108) X(112) X(120) X(128) X(144) X(160)
 
 bool size_supported(int N) {
     switch (N) {
@@ -259,25 +262,50 @@ void launch_voxels(md_ctx *c, const float *rot, float *vr, float *vi) {
     }
 }
 
-void launch_dock(md_ctx *c, int lane, cudaStream_t s, const float *rot, int nb, int rot0, int t, DevPose *pose,
-                 cudaEvent_t *ev = nullptr) {
+void launch_dock_ws(md_ctx *c, const WorkSet &w, cudaStream_t s, const float *rot, int nb, int rot0, int t,
+                    DevPose *pose, cudaEvent_t *ev = nullptr) {
     switch (c->N) {
 #define X(n) \
-    case n: Sized<n>::dock(c, c->ws[lane], s, rot, nb, rot0, t, pose, ev); break;
+    case n: Sized<n>::dock(c, w, s, rot, nb, rot0, t, pose, ev); break;
         MDB_SIZES(X)
 #undef X
     }
 }
 
+void launch_dock(md_ctx *c, int lane, cudaStream_t s, const float *rot, int nb, int rot0, int t, DevPose *pose,
+                 cudaEvent_t *ev = nullptr) {
+    launch_dock_ws(c, c->ws[lane], s, rot, nb, rot0, t, pose, ev);
+}
+
 void free_graphs(md_ctx *c) {
     for (auto &kv : c->graphs) cudaGraphExecDestroy(kv.second);
     c->graphs.clear();
+    for (auto &kv : c->pair_graphs) cudaGraphExecDestroy(kv.second);
+    c->pair_graphs.clear();
 }
 
 void release_work(md_ctx *c) {
     free_graphs(c);
     for (auto &w : c->ws) w.release();
     c->cap = c->cap_t = c->cap_na = 0;
+    c->have = WorkSet::Sizes{};
+}
+
+// Work sets holding at least `z` bytes per buffer.
+int ensure_bytes(md_ctx *ctx, const WorkSet::Sizes &z) {
+    bool ok = true;
+    for (int k = 0; k < 10; ++k) ok = ok && z.b[k] <= ctx->have.b[k];
+    if (ok) return MD_OK;
+    WorkSet::Sizes m = ctx->have;
+    for (int k = 0; k < 10; ++k) m.b[k] = std::max(m.b[k], z.b[k]);
+    const int cap = ctx->cap, t = ctx->cap_t, na = ctx->cap_na;
+    release_work(ctx);
+    for (auto &w : ctx->ws) MD_CUDA(w.allocate(m));
+    ctx->have = m;
+    ctx->cap = cap;
+    ctx->cap_t = t;
+    ctx->cap_na = na;
+    return MD_OK;
 }
 
 // Work sets for launch groups of `cap` rotations with t poses each.
@@ -286,8 +314,8 @@ int ensure_work(md_ctx *ctx, int cap, int t) {
     cap = std::max({cap, ctx->cap, 1});
     t = std::max({t, ctx->cap_t, 1});
     const int na = std::max({ctx->na, ctx->cap_na, 1});
-    release_work(ctx);
-    for (auto &w : ctx->ws) MD_CUDA(w.allocate(cap, ctx->N, t, na));
+    int rc = ensure_bytes(ctx, WorkSet::need(cap, ctx->N, t, na));
+    if (rc) return rc;
     ctx->cap = cap;
     ctx->cap_t = t;
     ctx->cap_na = na;
@@ -617,6 +645,73 @@ int md_dock_profile(md_ctx *ctx, const float *d_rot, int first_rot, int n_rot, i
     for (int k = 0; k < 5; ++k) stage_ms[k] = (float)acc[k];
     if (launches) *launches = nl;
     MD_CUDA(cudaGetLastError());
+    return MD_OK;
+}
+
+int md_dock_pairs(md_ctx *runner, md_ctx *const *pairs, int npairs, const float *const *d_rotmat, const int *n_rot,
+                  int t, md_pose *const *d_out) {
+    md_ctx *ctx = runner;
+    if (!ctx || !pairs || !d_rotmat || !n_rot || !d_out || npairs < 0 || t < 1) return MD_ERR_ARG;
+    MD_CUDA(cudaSetDevice(ctx->device));
+    // shared work sets: the largest launch group of any pair
+    WorkSet::Sizes z{};
+    std::vector<uintptr_t> key{(uintptr_t)npairs, (uintptr_t)t};
+    for (int p = 0; p < npairs; ++p) {
+        md_ctx *c = pairs[p];
+        if (!c || !d_rotmat[p] || !d_out[p] || n_rot[p] < 0) return MD_ERR_ARG;
+        if (c->device != ctx->device) {
+            ctx->err = "md_dock_pairs: pair " + std::to_string(p) + " is on another device";
+            return MD_ERR_ARG;
+        }
+        int rc = check_ready(c);
+        if (rc) {
+            ctx->err = "md_dock_pairs: pair " + std::to_string(p) + ": " + c->err;
+            return rc;
+        }
+        MD_CUDA(set_attrs(c->N));
+        const int B = std::max(1, std::min(c->batch, std::max(n_rot[p], 1)));
+        const WorkSet::Sizes zp = WorkSet::need(B, c->N, t, std::max(c->na, 1));
+        for (int k = 0; k < 10; ++k) z.b[k] = std::max(z.b[k], zp.b[k]);
+        key.insert(key.end(), {(uintptr_t)c, (uintptr_t)d_rotmat[p], (uintptr_t)n_rot[p], (uintptr_t)d_out[p],
+                               (uintptr_t)B, (uintptr_t)c->na, (uintptr_t)c->N});
+    }
+    int rc = ensure_bytes(ctx, z);
+    if (rc) return rc;
+    auto it = ctx->pair_graphs.find(key);
+    if (it == ctx->pair_graphs.end()) {
+        cudaGraph_t g;
+        MD_CUDA(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+        cudaEventRecord(ctx->fork, ctx->stream);
+        cudaStreamWaitEvent(ctx->side, ctx->fork, 0);
+        int group = 0;
+        for (int p = 0; p < npairs; ++p) {
+            md_ctx *c = pairs[p];
+            const int B = std::max(1, std::min(c->batch, std::max(n_rot[p], 1)));
+            DevPose *out = reinterpret_cast<DevPose *>(d_out[p]);
+            for (int r = 0; r < n_rot[p]; r += B, ++group) {
+                const int nb = std::min(B, n_rot[p] - r);
+                const int lane = group % kLanes;
+                launch_dock_ws(c, ctx->ws[lane], lane ? ctx->side : ctx->stream, d_rotmat[p] + 9 * (size_t)r, nb, r,
+                               t, out + (size_t)r * t);
+            }
+        }
+        cudaEventRecord(ctx->join, ctx->side);
+        cudaStreamWaitEvent(ctx->stream, ctx->join, 0);
+        cudaError_t ce = cudaStreamEndCapture(ctx->stream, &g);
+        if (ce != cudaSuccess) {
+            ctx->err = std::string("graph capture: ") + cudaGetErrorString(ce);
+            return MD_ERR_CUDA;
+        }
+        cudaGraphExec_t ex;
+        ce = cudaGraphInstantiate(&ex, g, 0);
+        cudaGraphDestroy(g);
+        if (ce != cudaSuccess) {
+            ctx->err = std::string("graph instantiate: ") + cudaGetErrorString(ce);
+            return MD_ERR_CUDA;
+        }
+        it = ctx->pair_graphs.emplace(key, ex).first;
+    }
+    MD_CUDA(cudaGraphLaunch(it->second, ctx->stream));
     return MD_OK;
 }
 

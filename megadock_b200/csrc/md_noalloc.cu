@@ -42,8 +42,8 @@ constexpr int kMaxN = 128;
 constexpr int kMaxT = 64;
 constexpr int kMaxDevices = 64;
 // twiddle tables for every supported N <= kMaxN, concatenated
-constexpr int kTwSizes[] = {32, 48, 64, 80, 96, 112, 120, 128};
-constexpr int kTwTotal = 32 + 48 + 64 + 80 + 96 + 112 + 120 + 128;
+constexpr int kTwSizes[] = {32, 48, 64, 72, 80, 96, 100, 108, 112, 120, 128};
+constexpr int kTwTotal = 32 + 48 + 64 + 72 + 80 + 96 + 100 + 108 + 112 + 120 + 128;
 
 static __device__ __align__(256) unsigned char g_scratch[kScratchBytes];
 static __device__ __align__(256) float2 g_twiddle[kTwTotal];
@@ -110,7 +110,7 @@ int setup(int dev) {
     cudaError_t e = cudaSuccess;
 #define X(n) \
     if (e == cudaSuccess) e = set_attrs<n>();
-    X(32) X(48) X(64) X(80) X(96) X(112) X(120) X(128)
+    X(32) X(48) X(64) X(72) X(80) X(96) X(100) X(108) X(112) X(120) X(128)
 #undef X
     if (e != cudaSuccess) return MD_ERR_CUDA;
     st.ready = true;
@@ -210,7 +210,7 @@ extern "C" int md_dock_noalloc(int nf1, float grid_width, const float *d_grid_co
         switch (nf1) {
 #define X(n) \
     case n: run_rotation<n>(s, L, G, rot9, Rh, prep, vbits, qlist, qcount, A, Gsp, cand, first_rot + r, t, pr); break;
-            X(32) X(48) X(64) X(80) X(96) X(112) X(120) X(128)
+            X(32) X(48) X(64) X(72) X(80) X(96) X(100) X(108) X(112) X(120) X(128)
 #undef X
         }
     }

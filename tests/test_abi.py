@@ -31,7 +31,7 @@ def test_cli_built(built):
 
 def test_kernel_sizes_built(built):
     from megadock_b200 import lib
-    for n in (64, 96, 128, 160):
+    for n in (32, 48, 64, 72, 80, 96, 100, 108, 112, 120, 128, 144, 160):
         assert lib().md_fft_size_supported(n) == 1
-    for n in (90, 100, 2048):
+    for n in (90, 98, 2048):
         assert lib().md_fft_size_supported(n) == 0
