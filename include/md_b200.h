@@ -108,6 +108,23 @@ int md_dock_pairs(md_ctx *runner, md_ctx *const *pairs, int npairs, const float 
 int md_dock_profile(md_ctx *ctx, const float *d_rotmat, int first_rot, int n_rot, int t, md_pose *d_out,
                     float *stage_ms, int *launches);
 
+/* Adjoint (no counterpart in the reference, whose scores are not
+ * differentiated): gradient of the smooth loss
+ *     L = T * log(sum_r exp(s_r / T))
+ * over the per-rotation top-1 scores s_r of the rotations in rotmat
+ * (9 * n_rot floats) whose poses top1[n_rot] came from md_dock with t = 1.
+ * Outputs (host buffers, any may be NULL): *loss; dL/d(receptor grid) real and
+ * imaginary parts d_rec_r/d_rec_i (ng1^3 each, the grids given to
+ * md_receptor_fft); dL/d(ligand atom charge) d_charge (na); dL/d(alpha)
+ * d_alpha, alpha being the electrostatic weight -e that scales the receptor's
+ * imaginary grid (its support held fixed); and, for the n_lig_rot rotations
+ * listed in lig_rot (indices into rotmat), dL/d(ligand grid) d_lig_r/d_lig_i
+ * (n_lig_rot * ng1^3 each).  Rotations whose top score was clamped to 0 carry
+ * no gradient.  FP32 accumulation in a fixed order. */
+int md_adjoint_lse(md_ctx *ctx, const float *rotmat, int n_rot, const md_pose *top1, float temperature, float alpha,
+                   double *loss, float *d_rec_r, float *d_rec_i, float *d_charge, double *d_alpha,
+                   const int *lig_rot, int n_lig_rot, float *d_lig_r, float *d_lig_i);
+
 /* Ligand::rpscace + Ligand::electro (src/ligand.cpp:20-239) of one rotation,
  * computed by the device voxelizer; grid_r/grid_i receive ng1^3 floats. */
 int md_ligand_voxels(md_ctx *ctx, const float *rotmat9, float *grid_r, float *grid_i);

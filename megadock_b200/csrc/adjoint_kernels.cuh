@@ -1,0 +1,101 @@
+// Adjoint of a smooth loss over the per-rotation top-1 scores (sm_100a).
+//
+// With s_r = score_r(t*_r) = sum_x Rr(x) Lr_r(x + t*_r) + Ri(x) Li_r(x + t*_r)
+// (circular FFT coordinates, src/fft_process.cpp:333-346 product + inverse
+// FFT) and dL/ds_r = w_r, the gradients are transposed correlations that
+// collapse to shifts at the selected translations:
+//   dL/dR(x)    = sum_r w_r L_r(x + t*_r)        (k_adj_receptor: gather, rotations in order)
+//   dL/dL_r(y)  = w_r R(y - t*_r)                (k_adj_ligand)
+//   dL/dq_a     = sum_r w_r Ri(c_r(a) - t*_r)    (k_adj_charge: through the charge-cell assignment)
+// Grids are the ng^3 voxel grids; their FFT embedding is at offset N/4 on each
+// axis (src/fft_process.cpp:306-330).  Accumulation is FP32 in a fixed order.
+#pragma once
+#include "dock_kernels.cuh"
+
+namespace mdb {
+
+// Voxel index of the embedded grid at FFT position (a + d) mod N, or -1 when
+// it falls in the zero padding.
+__device__ __forceinline__ int adj_cell(int a, int d, int N, int ng) {
+    const int off = N / 4;
+    int y = a + off + d;
+    y %= N;
+    if (y < 0) y += N;
+    y -= off;
+    return (y >= 0 && y < ng) ? y : -1;
+}
+
+// dRr/dRi += sum over the chunk's rotations of w_r * (Lr_r, Li_r)(x + t*_r).
+__global__ void k_adj_receptor(int N, int ng, int nb, const float *__restrict__ vr, const float *__restrict__ vi,
+                               const int4 *__restrict__ shift, const float *__restrict__ w, float *__restrict__ dRr,
+                               float *__restrict__ dRi) {
+    const size_t ng3 = (size_t)ng * ng * ng;
+    const size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= ng3) return;
+    const int i = (int)(c / ((size_t)ng * ng)), j = (int)((c / ng) % ng), k = (int)(c % ng);
+    float ar = dRr[c], ai = dRi[c];
+    for (int r = 0; r < nb; ++r) {
+        const float wr = __ldg(&w[r]);
+        if (wr == 0.f) continue;
+        const int4 t = __ldg(&shift[r]);
+        const int yi = adj_cell(i, t.x, N, ng), yj = adj_cell(j, t.y, N, ng), yk = adj_cell(k, t.z, N, ng);
+        if (yi < 0 || yj < 0 || yk < 0) continue;
+        const size_t y = (size_t)r * ng3 + ((size_t)yi * ng + yj) * ng + yk;
+        ar = fmaf(wr, __ldg(&vr[y]), ar);
+        ai = fmaf(wr, __ldg(&vi[y]), ai);
+    }
+    dRr[c] = ar;
+    dRi[c] = ai;
+}
+
+// dL/dL_r(y) = w_r * R(y - t*_r) for the selected rotations (sel[m] = r).
+__global__ void k_adj_ligand(int N, int ng, int nsel, const int *__restrict__ sel, const float *__restrict__ recr,
+                             const float *__restrict__ reci, const int4 *__restrict__ shift,
+                             const float *__restrict__ w, float *__restrict__ dLr, float *__restrict__ dLi) {
+    const size_t ng3 = (size_t)ng * ng * ng;
+    const size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int m = blockIdx.y;
+    if (c >= ng3 || m >= nsel) return;
+    const int r = sel[m];
+    const int i = (int)(c / ((size_t)ng * ng)), j = (int)((c / ng) % ng), k = (int)(c % ng);
+    const int4 t = shift[r];
+    const int xi = adj_cell(i, -t.x, N, ng), xj = adj_cell(j, -t.y, N, ng), xk = adj_cell(k, -t.z, N, ng);
+    float gr = 0.f, gi = 0.f;
+    if (xi >= 0 && xj >= 0 && xk >= 0 && w[r] != 0.f) {
+        const size_t x = ((size_t)xi * ng + xj) * ng + xk;
+        gr = w[r] * recr[x];
+        gi = w[r] * reci[x];
+    }
+    dLr[(size_t)m * ng3 + c] = gr;
+    dLi[(size_t)m * ng3 + c] = gi;
+}
+
+// dL/dq_a = sum_r w_r Ri(c_r(a) - t*_r), c_r(a) = the atom's charge cell in
+// rotation r (the same bit-exact rotation and cell rule as the voxelizer).
+__global__ void k_adj_charge(LigandView L, GridView G, int N, int n_rot, const float *__restrict__ rotm,
+                             const int4 *__restrict__ shift, const float *__restrict__ w,
+                             const float *__restrict__ reci, float *__restrict__ dq) {
+    const int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= L.na) return;
+    const float4 at = __ldg(&L.atom[a]);
+    const int ng = G.ng;
+    float acc = 0.f;
+    for (int r = 0; r < n_rot; ++r) {
+        const float wr = __ldg(&w[r]);
+        if (wr == 0.f) continue;
+        const float *m = rotm + 9 * (size_t)r;
+        float mm[9];
+#pragma unroll
+        for (int e = 0; e < 9; ++e) mm[e] = __ldg(&m[e]);
+        const int ci = charge_cell(rot_x(mm, at.x, at.y, at.z), G.pad, G.gw, ng);
+        const int cj = charge_cell(rot_x(mm + 3, at.x, at.y, at.z), G.pad, G.gw, ng);
+        const int ck = charge_cell(rot_x(mm + 6, at.x, at.y, at.z), G.pad, G.gw, ng);
+        const int4 t = __ldg(&shift[r]);
+        const int xi = adj_cell(ci, -t.x, N, ng), xj = adj_cell(cj, -t.y, N, ng), xk = adj_cell(ck, -t.z, N, ng);
+        if (xi < 0 || xj < 0 || xk < 0) continue;
+        acc = fmaf(wr, __ldg(&reci[((size_t)xi * ng + xj) * ng + xk]), acc);
+    }
+    dq[a] = acc;
+}
+
+}  // namespace mdb

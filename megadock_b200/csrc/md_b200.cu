@@ -22,6 +22,7 @@
 #include <vector>
 
 #include "../../include/md_b200.h"
+#include "adjoint_kernels.cuh"
 #include "dock_kernels.cuh"
 
 using namespace mdb;
@@ -90,8 +91,9 @@ struct md_ctx {
     float gw = 0.f;
     float *d_gc = nullptr;
     float2 *d_tw = nullptr;
-    // receptor spectrum [kx][ky][kz]
+    // receptor spectrum [kx][ky][kz] and the receptor voxel grids (for the adjoint)
     float2 *d_Rh = nullptr;
+    float *d_recv = nullptr;   // [2][ng^3] real, imaginary
     bool have_receptor = false;
     // ligand
     int na = 0, na_cap = 0;
@@ -176,6 +178,16 @@ struct Sized {
                                                     w.qcount);
     }
 
+    // Voxel grids of nb rotations ([nb][ng^3] real, imaginary) into vr / vi.
+    static void voxel_chunk(md_ctx *c, const float *d_rot9, int nb, float *d_vr, float *d_vi) {
+        GridView G{c->ng, c->gw, (float)(c->ng * c->gw) / 2, c->d_gc, c->d_tw};
+        LigandView L{c->na, c->d_atom, c->d_rad2, c->delta};
+        const WorkSet &w = c->ws[0];
+        voxelize(c, w, d_rot9, nb, c->stream);
+        k_plane_fwd<N, 2><<<dim3(NG, nb), kNT, smem_fwd(), c->stream>>>(L, G, w.vbits, w.qlist, w.qcount, nullptr,
+                                                                         nullptr, nullptr, d_vr, d_vi);
+    }
+
     static void voxels(md_ctx *c, const float *d_rot9, float *d_vr, float *d_vi) {
         GridView G{c->ng, c->gw, (float)(c->ng * c->gw) / 2, c->d_gc, c->d_tw};
         LigandView L{c->na, c->d_atom, c->d_rad2, c->delta};
@@ -248,6 +260,15 @@ void launch_receptor(md_ctx *c, const float *r, const float *i) {
     switch (c->N) {
 #define X(n) \
     case n: Sized<n>::receptor(c, r, i); break;
+        MDB_SIZES(X)
+#undef X
+    }
+}
+
+void launch_voxel_chunk(md_ctx *c, const float *rot, int nb, float *vr, float *vi) {
+    switch (c->N) {
+#define X(n) \
+    case n: Sized<n>::voxel_chunk(c, rot, nb, vr, vi); break;
         MDB_SIZES(X)
 #undef X
     }
@@ -422,6 +443,7 @@ void md_ctx_destroy(md_ctx *ctx) {
     cudaFree(ctx->d_gc);
     cudaFree(ctx->d_tw);
     cudaFree(ctx->d_Rh);
+    cudaFree(ctx->d_recv);
     cudaFree(ctx->d_atom);
     cudaFree(ctx->d_rad2);
     cudaFree(ctx->d_rot);
@@ -455,14 +477,17 @@ int md_set_grid(md_ctx *ctx, int nf1, float grid_width, const float *grid_coord)
         cudaFree(ctx->d_gc);
         cudaFree(ctx->d_tw);
         cudaFree(ctx->d_Rh);
+        cudaFree(ctx->d_recv);
         ctx->d_gc = nullptr;
         ctx->d_tw = nullptr;
         ctx->d_Rh = nullptr;
+        ctx->d_recv = nullptr;
         ctx->have_receptor = false;
         const size_t N = nf1;
         MD_CUDA(cudaMalloc(&ctx->d_gc, sizeof(float) * N / 2));
         MD_CUDA(cudaMalloc(&ctx->d_tw, sizeof(float2) * N));
         MD_CUDA(cudaMalloc(&ctx->d_Rh, sizeof(float2) * N * N * N));
+        MD_CUDA(cudaMalloc(&ctx->d_recv, sizeof(float) * 2 * (N / 2) * (N / 2) * (N / 2)));
         std::vector<float2> tw(N);
         for (size_t j = 0; j < N; ++j) {
             const double a = -2.0 * M_PI * (double)j / (double)N;
@@ -490,15 +515,12 @@ int md_receptor_fft(md_ctx *ctx, const float *grid_r, const float *grid_i) {
     int rc = ensure_work(ctx, std::max(1, ctx->batch), 1);
     if (rc) return rc;
     const size_t ng3 = (size_t)ctx->ng * ctx->ng * ctx->ng;
-    float *d_r = nullptr, *d_i = nullptr;
-    MD_CUDA(cudaMalloc(&d_r, sizeof(float) * ng3 * 2));
-    d_i = d_r + ng3;
+    float *d_r = ctx->d_recv, *d_i = ctx->d_recv + ng3;
     MD_CUDA(cudaMemcpyAsync(d_r, grid_r, sizeof(float) * ng3, cudaMemcpyHostToDevice, ctx->stream));
     MD_CUDA(cudaMemcpyAsync(d_i, grid_i, sizeof(float) * ng3, cudaMemcpyHostToDevice, ctx->stream));
     launch_receptor(ctx, d_r, d_i);
     cudaError_t e = cudaGetLastError();
     if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
-    cudaFree(d_r);
     if (e != cudaSuccess) {
         ctx->err = std::string("receptor FFT: ") + cudaGetErrorString(e);
         return MD_ERR_CUDA;
@@ -712,6 +734,121 @@ int md_dock_pairs(md_ctx *runner, md_ctx *const *pairs, int npairs, const float 
         it = ctx->pair_graphs.emplace(key, ex).first;
     }
     MD_CUDA(cudaGraphLaunch(it->second, ctx->stream));
+    return MD_OK;
+}
+
+int md_adjoint_lse(md_ctx *ctx, const float *rotmat, int n_rot, const md_pose *top1, float temperature, float alpha,
+                   double *loss, float *d_rec_r, float *d_rec_i, float *d_charge, double *d_alpha,
+                   const int *lig_rot, int n_lig_rot, float *d_lig_r, float *d_lig_i) {
+    if (!ctx || !rotmat || !top1 || n_rot < 1 || !(temperature > 0.f)) return MD_ERR_ARG;
+    if (n_lig_rot > 0 && (!lig_rot || !d_lig_r || !d_lig_i)) return MD_ERR_ARG;
+    int rc = check_ready(ctx);
+    if (rc) return rc;
+    MD_CUDA(cudaSetDevice(ctx->device));
+    const int N = ctx->N, ng = ctx->ng;
+    const size_t ng3 = (size_t)ng * ng * ng;
+    // loss and weights in double on the host: w_r = softmax(s_r / T); rotations
+    // whose score was clamped to 0 (no positive cell) have no parameter gradient
+    double smax = -1e300;
+    for (int r = 0; r < n_rot; ++r) smax = std::max(smax, (double)top1[r].score);
+    double z = 0.0;
+    for (int r = 0; r < n_rot; ++r) z += std::exp(((double)top1[r].score - smax) / temperature);
+    if (loss) *loss = smax + temperature * std::log(z);
+    std::vector<float> w(n_rot);
+    std::vector<int4> shift(n_rot);
+    for (int r = 0; r < n_rot; ++r) {
+        const bool live = top1[r].score > 0.f;
+        w[r] = live ? (float)(std::exp(((double)top1[r].score - smax) / temperature) / z) : 0.f;
+        shift[r] = make_int4(top1[r].i, top1[r].j, top1[r].k, 0);
+    }
+    const int B = std::max(1, std::min(ctx->batch, n_rot));
+    if ((rc = ensure_work(ctx, B, 1))) return rc;
+    // device scratch of this call
+    float *d_rot = nullptr, *d_w = nullptr, *d_grad = nullptr, *d_vox = nullptr, *d_dq = nullptr;
+    int4 *d_shift = nullptr;
+    auto cleanup = [&]() {
+        cudaFree(d_rot);
+        cudaFree(d_w);
+        cudaFree(d_grad);
+        cudaFree(d_vox);
+        cudaFree(d_dq);
+        cudaFree(d_shift);
+    };
+    auto fail = [&](cudaError_t e) {
+        ctx->err = std::string("adjoint: ") + cudaGetErrorString(e);
+        cleanup();
+        return MD_ERR_CUDA;
+    };
+    cudaError_t e = cudaSuccess;
+    if (e == cudaSuccess) e = cudaMalloc(&d_rot, sizeof(float) * 9 * n_rot);
+    if (e == cudaSuccess) e = cudaMalloc(&d_w, sizeof(float) * n_rot);
+    if (e == cudaSuccess) e = cudaMalloc(&d_shift, sizeof(int4) * n_rot);
+    if (e == cudaSuccess) e = cudaMalloc(&d_grad, sizeof(float) * 2 * ng3);
+    if (e == cudaSuccess) e = cudaMalloc(&d_vox, sizeof(float) * 2 * ng3 * B);
+    if (e == cudaSuccess) e = cudaMalloc(&d_dq, sizeof(float) * std::max(ctx->na, 1));
+    if (e != cudaSuccess) return fail(e);
+    cudaStream_t s = ctx->stream;
+    cudaMemcpyAsync(d_rot, rotmat, sizeof(float) * 9 * n_rot, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(d_w, w.data(), sizeof(float) * n_rot, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(d_shift, shift.data(), sizeof(int4) * n_rot, cudaMemcpyHostToDevice, s);
+    cudaMemsetAsync(d_grad, 0, sizeof(float) * 2 * ng3, s);
+    const int thr = 256;
+    const int blocks = (int)((ng3 + thr - 1) / thr);
+    // receptor gradient: voxel grids of each chunk of rotations, then the gather
+    for (int r0 = 0; r0 < n_rot; r0 += B) {
+        const int nb = std::min(B, n_rot - r0);
+        launch_voxel_chunk(ctx, d_rot + 9 * (size_t)r0, nb, d_vox, d_vox + ng3 * B);
+        k_adj_receptor<<<blocks, thr, 0, s>>>(N, ng, nb, d_vox, d_vox + ng3 * B, d_shift + r0, d_w + r0, d_grad,
+                                              d_grad + ng3);
+    }
+    // charge gradient through the charge-cell assignment
+    GridView G{ng, ctx->gw, (float)(ng * ctx->gw) / 2, ctx->d_gc, ctx->d_tw};
+    LigandView L{ctx->na, ctx->d_atom, ctx->d_rad2, ctx->delta};
+    k_adj_charge<<<(ctx->na + 127) / 128, 128, 0, s>>>(L, G, N, n_rot, d_rot, d_shift, d_w, ctx->d_recv + ng3, d_dq);
+    if ((e = cudaGetLastError()) != cudaSuccess) return fail(e);
+    std::vector<float> gr(ng3), gi(ng3);
+    if ((e = cudaMemcpyAsync(gr.data(), d_grad, sizeof(float) * ng3, cudaMemcpyDeviceToHost, s)) != cudaSuccess)
+        return fail(e);
+    if ((e = cudaMemcpyAsync(gi.data(), d_grad + ng3, sizeof(float) * ng3, cudaMemcpyDeviceToHost, s)) != cudaSuccess)
+        return fail(e);
+    if (d_charge &&
+        (e = cudaMemcpyAsync(d_charge, d_dq, sizeof(float) * ctx->na, cudaMemcpyDeviceToHost, s)) != cudaSuccess)
+        return fail(e);
+    // ligand-grid gradient of the selected rotations
+    if (n_lig_rot > 0) {
+        int *d_sel = nullptr;
+        float *d_lg = nullptr;
+        if ((e = cudaMalloc(&d_sel, sizeof(int) * n_lig_rot)) != cudaSuccess) return fail(e);
+        if ((e = cudaMalloc(&d_lg, sizeof(float) * 2 * ng3 * n_lig_rot)) != cudaSuccess) {
+            cudaFree(d_sel);
+            return fail(e);
+        }
+        cudaMemcpyAsync(d_sel, lig_rot, sizeof(int) * n_lig_rot, cudaMemcpyHostToDevice, s);
+        k_adj_ligand<<<dim3(blocks, n_lig_rot), thr, 0, s>>>(N, ng, n_lig_rot, d_sel, ctx->d_recv, ctx->d_recv + ng3,
+                                                             d_shift, d_w, d_lg, d_lg + ng3 * n_lig_rot);
+        e = cudaMemcpyAsync(d_lig_r, d_lg, sizeof(float) * ng3 * n_lig_rot, cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(d_lig_i, d_lg + ng3 * n_lig_rot, sizeof(float) * ng3 * n_lig_rot,
+                                cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        cudaFree(d_sel);
+        cudaFree(d_lg);
+        if (e != cudaSuccess) return fail(e);
+    }
+    if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return fail(e);
+    if (d_rec_r) std::copy(gr.begin(), gr.end(), d_rec_r);
+    if (d_rec_i) std::copy(gi.begin(), gi.end(), d_rec_i);
+    if (d_alpha) {
+        // the receptor's imaginary grid is alpha times a fixed-support unit grid
+        std::vector<float> ri(ng3);
+        if ((e = cudaMemcpy(ri.data(), ctx->d_recv + ng3, sizeof(float) * ng3, cudaMemcpyDeviceToHost)) !=
+            cudaSuccess)
+            return fail(e);
+        double acc = 0.0;
+        for (size_t x = 0; x < ng3; ++x) acc += (double)gi[x] * (double)ri[x];
+        *d_alpha = alpha != 0.f ? acc / alpha : std::nan("");
+    }
+    cleanup();
     return MD_OK;
 }
 

@@ -63,6 +63,7 @@ class FFTProcess:
         q = np.ascontiguousarray(charge, dtype=np.float32)
         _check(N.lib().md_ligand_data(self._h, len(rad), N.fptr(xyz), N.fptr(rad), N.fptr(q), float(lig_core)),
                self._h)
+        self._na = len(rad)
 
     def set_batch(self, rotations_per_launch: int):
         _check(N.lib().md_set_batch(self._h, int(rotations_per_launch)), self._h)
@@ -95,6 +96,39 @@ class FFTProcess:
         i = np.zeros(ng ** 3, np.float32)
         _check(N.lib().md_ligand_voxels(self._h, N.fptr(m), N.fptr(r), N.fptr(i)), self._h)
         return r.reshape((ng,) * 3), i.reshape((ng,) * 3)
+
+    def adjoint_lse(self, rotmats: np.ndarray, top1: np.ndarray, temperature: float = 10.0, alpha: float = 1.0,
+                    lig_rot=()):
+        """Gradient of T*log(sum_r exp(s_r/T)) over the top-1 scores s_r of
+        md_dock (t = 1) poses.  Returns a dict: loss, d_rec_r, d_rec_i (ng^3),
+        d_charge (na), d_alpha and, for the rotation indices in lig_rot,
+        d_lig_r / d_lig_i (len(lig_rot), ng, ng, ng)."""
+        m = np.ascontiguousarray(rotmats, dtype=np.float32).reshape(-1, 9)
+        top1 = np.ascontiguousarray(top1).view(N.POSE_DTYPE).reshape(-1)
+        if len(top1) != len(m):
+            raise ValueError("one top-1 pose per rotation")
+        ng = self.num_fft // 2
+        ng3 = ng ** 3
+        na = self._na
+        sel = np.ascontiguousarray(lig_rot, dtype=np.int32).reshape(-1)
+        if sel.size and (sel.min() < 0 or sel.max() >= len(m)):
+            raise ValueError("lig_rot index out of range")
+        loss = C.c_double()
+        dalpha = C.c_double()
+        drr = np.zeros(ng3, np.float32)
+        dri = np.zeros(ng3, np.float32)
+        dq = np.zeros(max(na, 1), np.float32)
+        dlr = np.zeros(max(sel.size, 1) * ng3, np.float32)
+        dli = np.zeros(max(sel.size, 1) * ng3, np.float32)
+        _check(N.lib().md_adjoint_lse(self._h, N.fptr(m), len(m), N.vptr(top1), float(temperature), float(alpha),
+                                      C.byref(loss), N.fptr(drr), N.fptr(dri), N.fptr(dq), C.byref(dalpha),
+                                      sel.ctypes.data_as(C.POINTER(C.c_int)), int(sel.size), N.fptr(dlr),
+                                      N.fptr(dli)), self._h)
+        shape = (ng,) * 3
+        return {"loss": loss.value, "d_rec_r": drr.reshape(shape), "d_rec_i": dri.reshape(shape),
+                "d_charge": dq[:na], "d_alpha": dalpha.value,
+                "d_lig_r": dlr[:sel.size * ng3].reshape((sel.size,) + shape),
+                "d_lig_i": dli[:sel.size * ng3].reshape((sel.size,) + shape)}
 
     # -- FFTProcess::sort_index / top_score / top_index
     def sort_index(self, nout: int):

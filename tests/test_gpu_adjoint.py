@@ -1,0 +1,169 @@
+"""Device adjoint (md_adjoint_lse) on the GPU.
+
+Workload: the 150/70-residue pair at N = 96, 3,600 rotations, loss =
+log-sum-exp at temperature 10 of the per-rotation top-1 scores (float32
+forward, FP32-accumulated adjoint).  Checked
+  * against the FP64 reference gradient (oracle/adjoint.py) taken at the
+    device's own translations and scores: max-norm error per output below
+    1e-5 of the output's largest entry;
+  * against FP64 central finite differences of step 1e-3 on 200 random
+    coordinates (receptor grid values, ligand grid values of the four
+    heaviest rotations, per-atom charges, alpha): relative error <= 1e-3 at
+    every coordinate where the loss is differentiable within the step;
+  * through a torch.autograd.Function wrapper (tests/adjoint_fn.py).
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+T = 10.0
+H = 1e-3
+
+
+def _setup(pairs, name, *extra):
+    from megadock_b200 import FFTProcess, Job
+    rp, lp = pairs[name]
+    job = Job(["-R", rp, "-L", lp, *extra])
+    fp = FFTProcess(0)
+    fp.alloc_array(job.nf1, job.grid_width, job.grid_coord())
+    rr, ri = job.receptor_grids()
+    fp.receptor_fft(rr, ri)
+    xyz, rad, q = job.ligand_atoms()
+    fp.ligand_data_transfer_gpu(xyz, rad, q, job.lig_core)
+    return job, fp
+
+
+def _pick(rng, arr, k):
+    """k random entries among those whose gradient is at least 1e-4 of the
+    largest (smaller ones are below what an FP64 difference of the loss at
+    step 1e-3 resolves)."""
+    a = np.abs(arr).reshape(-1)
+    nz = np.flatnonzero(a >= 1e-4 * a.max())
+    return rng.choice(nz, min(k, len(nz)), replace=False)
+
+
+@pytest.fixture(scope="module")
+def adjoint_case(built, gpu, pairs):
+    from megadock_b200 import rotation_matrices
+    from oracle import adjoint as A
+    job, fp = _setup(pairs, "c0", "-F", "96", "-r", "3600")
+    mats = rotation_matrices(job.rotation_angles())
+    fp.set_batch(64)
+    top1 = fp.cuda_fft(mats, t=1).copy()
+    shifts = np.stack([top1["i"], top1["j"], top1["k"]], -1).astype(np.int64)
+    scores = top1["score"].astype(np.float64)
+    _, w = A.weights(scores, T)
+    lig_rot = np.argsort(-w)[:4]
+    dev = fp.adjoint_lse(mats, top1, T, 1.0, lig_rot=lig_rot)
+    rng = np.random.default_rng(2024)
+    rec = [(0, x) for x in _pick(rng, dev["d_rec_r"], 60)] + [(1, x) for x in _pick(rng, dev["d_rec_i"], 60)]
+    atoms = _pick(rng, dev["d_charge"], 40)
+    lig = []
+    for m, r in enumerate(lig_rot):
+        for p, key in ((0, "d_lig_r"), (1, "d_lig_i")):
+            lig += [(r, p, y) for y in _pick(rng, dev[key][m], 5)]
+    lig = lig[:200 - len(rec) - len(atoms) - 1]
+    coords = A.Coordinates(rec, atoms, lig, alpha=True)
+    assert len(coords) == 200
+    rr, ri = job.receptor_grids()
+    xyz, rad, q = job.ligand_atoms()
+    ref = A.AdjointReference(rr, ri, xyz, rad, q, job.grid_width, job.grid_coord(), job.lig_core, job.nf1,
+                             fft=A.TorchFFT("cuda:0"))
+    out = ref.run(mats, shifts, scores, T, 1.0, lig_rot=lig_rot, coords=coords, h=H)
+    return dict(job=job, fp=fp, mats=mats, top1=top1, shifts=shifts, scores=scores, lig_rot=lig_rot, dev=dev,
+                coords=coords, ref=out, ri=ri)
+
+
+def test_adjoint_vs_fp64_reference_gradient(adjoint_case):
+    c = adjoint_case
+    dev, ref = c["dev"], c["ref"]
+    assert abs(dev["loss"] - ref["loss"]) <= 1e-12 * abs(ref["loss"])
+    for key in ("d_rec_r", "d_rec_i", "d_charge"):
+        d = np.abs(dev[key].astype(np.float64) - ref[key]).max()
+        print(f"\nadjoint {key}: max |device - FP64| / max |FP64| = {d / np.abs(ref[key]).max():.3g}")
+        assert d <= 1e-5 * np.abs(ref[key]).max(), (key, d, np.abs(ref[key]).max())
+    for m, r in enumerate(c["lig_rot"]):
+        for p, key in ((0, "d_lig_r"), (1, "d_lig_i")):
+            want = ref["d_lig"][r][p]
+            assert np.abs(dev[key][m] - want).max() <= 1e-6 * max(np.abs(want).max(), 1e-30)
+    assert abs(dev["d_alpha"] - ref["d_alpha"]) <= 1e-5 * abs(ref["d_alpha"])
+
+
+def test_adjoint_vs_fp64_finite_differences(adjoint_case):
+    c = adjoint_case
+    fd_tab = c["ref"]["fd"]
+    scores = c["scores"]
+    # FP64 top scores agree with the device's within the forward tolerance
+    live = scores > 0
+    assert np.all(np.abs(fd_tab.top[live] - scores[live]) <= 1e-4 * np.abs(fd_tab.top[live]) + 1e-3)
+    # rotations whose FP64 maximiser differs from the device's (near ties) are
+    # left out of the loss on both sides
+    keep = (fd_tab.arg == c["shifts"]).all(1) | ~live
+    assert keep.mean() > 0.99
+    fd, ok = fd_tab.gradient(keep, H, T)
+    lig_keep = [int(r) for r in c["lig_rot"] if keep[int(r)]]
+    if keep.all():
+        dev = c["dev"]
+    else:
+        sub = np.flatnonzero(keep)
+        remap = {int(r): m for m, r in enumerate(sub)}
+        dev = c["fp"].adjoint_lse(c["mats"][sub], c["top1"][sub], T, 1.0, lig_rot=[remap[r] for r in lig_keep])
+    pos = {r: m for m, r in enumerate(lig_keep)}
+    co = c["coords"]
+    an = [(dev["d_rec_r"] if p == 0 else dev["d_rec_i"]).reshape(-1)[x] for p, x in co.rec]
+    an += list(dev["d_charge"][co.atoms])
+    valid = [True] * (len(co.rec) + len(co.atoms))
+    for r, p, y in co.lig:
+        valid.append(r in pos)
+        an.append((dev["d_lig_r"] if p == 0 else dev["d_lig_i"])[pos[r]].reshape(-1)[y] if r in pos else 0.0)
+    an.append(dev["d_alpha"])
+    valid.append(True)
+    an = np.asarray(an, np.float64)
+    sel = ok & np.asarray(valid)
+    assert sel.sum() >= 190, (ok.sum(), sum(valid))
+    rel = np.abs(an[sel] - fd[sel]) / np.abs(fd[sel])
+    print(f"\nadjoint vs FP64 finite differences: {sel.sum()} of {len(sel)} coordinates, "
+          f"{int((~keep).sum())} tied rotations left out, max relative error {rel.max():.3g}, "
+          f"median {np.median(rel):.3g}")
+    assert rel.max() <= 1e-3, (rel.max(), np.argmax(rel))
+
+
+def test_autograd_function_wrapper(built, gpu, pairs):
+    import torch
+
+    from adjoint_fn import LSEDock
+    from megadock_b200 import rotation_matrices
+    job, fp = _setup(pairs, "small", "-F", "64", "-r", "360")
+    mats = rotation_matrices(job.rotation_angles())
+    rr, ri = job.receptor_grids()
+    xyz, rad, q = job.ligand_atoms()
+    rec_r = torch.tensor(rr, requires_grad=True)
+    rec_u = torch.tensor(ri, requires_grad=True)            # the -e 1.0 grid: alpha * rec_u with alpha = 1
+    charge = torch.tensor(q, requires_grad=True)
+    alpha = torch.tensor(1.0, dtype=torch.float64, requires_grad=True)
+    loss = LSEDock.apply(rec_r, rec_u, charge, alpha, fp, job, mats, T)
+    loss.backward()
+    top1 = fp.cuda_fft(mats, t=1)
+    res = fp.adjoint_lse(mats, top1, T, 1.0)
+    assert float(loss.detach()) == res["loss"]
+    assert np.array_equal(rec_r.grad.numpy(), res["d_rec_r"])
+    assert np.array_equal(charge.grad.numpy(), res["d_charge"])
+    assert float(alpha.grad) == res["d_alpha"]
+    # gradient step on alpha changes the loss in the predicted direction
+    step = 1e-2 * np.sign(float(alpha.grad))
+    loss2 = LSEDock.apply(rec_r, rec_u, charge, alpha.detach() + step, fp, job, mats, T)
+    assert float(loss2.detach()) > float(loss.detach())
+
+
+def test_adjoint_rejects_bad_arguments(built, gpu, pairs):
+    from megadock_b200 import MdError, rotation_matrices
+    job, fp = _setup(pairs, "small", "-F", "64", "-r", "24")
+    mats = rotation_matrices(job.rotation_angles())
+    top1 = fp.cuda_fft(mats, t=1)
+    with pytest.raises(MdError):
+        fp.adjoint_lse(mats, top1, 0.0, 1.0)
+    with pytest.raises(ValueError):
+        fp.adjoint_lse(mats, top1[:3], T, 1.0)
+    with pytest.raises(ValueError):
+        fp.adjoint_lse(mats, top1, T, 1.0, lig_rot=[24])
