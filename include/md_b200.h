@@ -125,6 +125,22 @@ int md_adjoint_lse(md_ctx *ctx, const float *rotmat, int n_rot, const md_pose *t
                    double *loss, float *d_rec_r, float *d_rec_i, float *d_charge, double *d_alpha,
                    const int *lig_rot, int n_lig_rot, float *d_lig_r, float *d_lig_i);
 
+/* General form of the adjoint: dL/d(parameters) for a loss whose gradient
+ * with respect to the scores of n poses is dl_ds[n] (host floats).  Pose p
+ * has the rotation rotmat[9p..9p+8] and the translation (i, j, k) of
+ * poses[p] (the score and rot fields are not read).  Outputs as for
+ * md_adjoint_lse; lig_pose[n_lig] lists poses (indices into the n) whose
+ * ligand-grid gradient is wanted.  md_adjoint_lse is this with
+ * dl_ds = softmax(s / T). */
+int md_adjoint_poses(md_ctx *ctx, const float *rotmat, int n, const md_pose *poses, const float *dl_ds,
+                     float *d_rec_r, float *d_rec_i, float *d_charge, const int *lig_pose, int n_lig,
+                     float *d_lig_r, float *d_lig_i);
+
+/* Scores of given poses (rotation rotmat[9p..], translation poses[p].i/j/k)
+ * formed directly as sum_x Rr(x) Lr(x + t) + Ri(x) Li(x + t): the value of the
+ * score grid at that translation (FP32, fixed summation order). */
+int md_pose_scores(md_ctx *ctx, const float *rotmat, int n, const md_pose *poses, float *scores);
+
 /* Ligand::rpscace + Ligand::electro (src/ligand.cpp:20-239) of one rotation,
  * computed by the device voxelizer; grid_r/grid_i receive ng1^3 floats. */
 int md_ligand_voxels(md_ctx *ctx, const float *rotmat9, float *grid_r, float *grid_i);
@@ -182,6 +198,13 @@ int md_job_grid_coord(const md_job *job, float *out);                 /* ng1 */
 int md_job_receptor_grids(const md_job *job, float *grid_r, float *grid_i); /* ng1^3 */
 int md_job_ligand_atoms(const md_job *job, float *xyz_centred, float *radius, float *charge);
 int md_job_receptor_atoms(const md_job *job, float *xyz, float *radius, float *charge, float *ace);
+/* Receptor::electro (src/receptor.cpp:258-346) split by atom group: grids
+ * holds ngroups * ng1^3 floats; atom l adds its field to grid group[l]
+ * (atoms with group[l] outside [0, ngroups) are left out).  Same search
+ * radius, dielectric, core mask and electrostatic ratio as the job's
+ * receptor grid, so the groups sum to md_job_receptor_grids' imaginary part
+ * up to the order of the float additions. */
+int md_job_receptor_elec_groups(const md_job *job, const int *group, int ngroups, float *grids);
 int md_job_centers(const md_job *job, float *rec_center, float *lig_center);
 int md_job_rotation_angles(const md_job *job, float *theta);         /* 3 * n_rot */
 float md_job_lig_core(const md_job *job);

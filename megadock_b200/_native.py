@@ -53,6 +53,8 @@ _PROTOS = {
     "md_dock_pairs": (C.c_int, [_VP, C.POINTER(_VP), C.c_int, C.POINTER(_VP), C.POINTER(C.c_int), C.c_int,
                                 C.POINTER(_VP)]),
     "md_ligand_voxels": (C.c_int, [_VP, _FP, _FP, _FP]),
+    "md_adjoint_poses": (C.c_int, [_VP, _FP, C.c_int, _VP, _FP, _FP, _FP, _FP, _IP, C.c_int, _FP, _FP]),
+    "md_pose_scores": (C.c_int, [_VP, _FP, C.c_int, _VP, _FP]),
     "md_adjoint_lse": (C.c_int, [_VP, _FP, C.c_int, _VP, C.c_float, C.c_float, C.POINTER(C.c_double), _FP, _FP, _FP,
                                  C.POINTER(C.c_double), _IP, C.c_int, _FP, _FP]),
     "md_dock_profile": (C.c_int, [_VP, _VP, C.c_int, C.c_int, C.c_int, _VP, _FP, _IP]),
@@ -72,6 +74,7 @@ _PROTOS = {
     "md_job_receptor_grids": (C.c_int, [_VP, _FP, _FP]),
     "md_job_ligand_atoms": (C.c_int, [_VP, _FP, _FP, _FP]),
     "md_job_receptor_atoms": (C.c_int, [_VP, _FP, _FP, _FP, _FP]),
+    "md_job_receptor_elec_groups": (C.c_int, [_VP, _IP, C.c_int, _FP]),
     "md_job_centers": (C.c_int, [_VP, _FP, _FP]),
     "md_job_rotation_angles": (C.c_int, [_VP, _FP]),
     "md_job_lig_core": (C.c_float, [_VP]),

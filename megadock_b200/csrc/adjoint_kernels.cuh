@@ -98,4 +98,37 @@ __global__ void k_adj_charge(LigandView L, GridView G, int N, int n_rot, const f
     dq[a] = acc;
 }
 
+// Score of one pose per block: sum_x Rr(x) Lr(x + t) + Ri(x) Li(x + t) over the
+// receptor grid (the value the inverse FFT gives at translation t, formed
+// directly).  Per-thread float sums in a fixed stride order, then a fixed
+// shuffle tree, so the result does not depend on scheduling.
+__global__ void k_pose_dot(int N, int ng, const float *__restrict__ recr, const float *__restrict__ reci,
+                           const float *__restrict__ vr, const float *__restrict__ vi,
+                           const int4 *__restrict__ shift, float *__restrict__ score) {
+    __shared__ float part[32];
+    const size_t ng3 = (size_t)ng * ng * ng;
+    const int b = blockIdx.x;
+    const int4 t = shift[b];
+    const float *lr = vr + (size_t)b * ng3, *li = vi + (size_t)b * ng3;
+    float acc = 0.f;
+    for (size_t c = threadIdx.x; c < ng3; c += blockDim.x) {
+        const int i = (int)(c / ((size_t)ng * ng)), j = (int)((c / ng) % ng), k = (int)(c % ng);
+        const int yi = adj_cell(i, t.x, N, ng), yj = adj_cell(j, t.y, N, ng), yk = adj_cell(k, t.z, N, ng);
+        if (yi < 0 || yj < 0 || yk < 0) continue;
+        const size_t y = ((size_t)yi * ng + yj) * ng + yk;
+        acc = fmaf(recr[c], lr[y], acc);
+        acc = fmaf(reci[c], li[y], acc);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        float v = threadIdx.x < (blockDim.x >> 5) ? part[threadIdx.x] : 0.f;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (threadIdx.x == 0) score[b] = v;
+    }
+}
+
 }  // namespace mdb

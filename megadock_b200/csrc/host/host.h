@@ -70,6 +70,13 @@ std::vector<float> centred_coordinates(const Molecule &m);
 void receptor_grids(const Molecule &rec, const Params &p, const std::vector<float> &gc, int ng1,
                     std::vector<float> &grid_r, std::vector<float> &grid_i);
 
+// The electrostatic part alone (src/receptor.cpp:258-346) over the receptor
+// core mask grid_r, into ngroups grids of ng1^3 (out): atom l contributes to
+// grid group[l] (skipped when outside [0, ngroups)); group == nullptr puts
+// every atom in grid 0, which is then the receptor's imaginary grid.
+void receptor_electro(const Molecule &rec, const Params &p, const std::vector<float> &gc, int ng1,
+                      const std::vector<float> &grid_r, const int *group, int ngroups, float *out);
+
 // Rotation matrix of Docking::ligand_rotationz (src/docking.cpp:376-384).
 void rotation_matrix(const float *theta, float *m9);
 

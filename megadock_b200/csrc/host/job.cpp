@@ -146,6 +146,12 @@ int md_job_receptor_grids(const md_job *job, float *r, float *i) {
     return MD_OK;
 }
 
+int md_job_receptor_elec_groups(const md_job *job, const int *group, int ngroups, float *grids) {
+    if (!job || !group || ngroups < 1 || !grids) return MD_ERR_ARG;
+    receptor_electro(job->rec, job->p, job->gc, job->ng1, job->rec_r, group, ngroups, grids);
+    return MD_OK;
+}
+
 int md_job_ligand_atoms(const md_job *job, float *xyz, float *radius, float *charge) {
     if (!job) return MD_ERR_ARG;
     if (xyz) std::copy(job->lig_xyz.begin(), job->lig_xyz.end(), xyz);

@@ -121,38 +121,54 @@ void receptor_grids(const Molecule &rec, const Params &p, const std::vector<floa
     for (size_t c = 0; c < ng3; ++c)
         if (grid_r[c] != epsilon) grid_r[c] = shell[c];
 
-    // electrostatics
-    {
-        const float beta = -2800.0f;
-        const float e_ratio = p.elec_ratio;
-        const float width = gc[1] - gc[0];
-        const float charge_per_grid = -1 * width * 80.0f / (beta * e_ratio);
-        auto origin_w = [&](float c) { return (int)(c / width + ng1 / 2); };
-        for (int l = 0; l < na; ++l) {
-            const float q = rec.charge[l];
-            const float aq = std::fabs(q);
-            if (aq <= 1.0e-6f) continue;
-            int reach;
-            if (aq < 0.07) reach = 4;
-            else if (aq < 0.21) reach = 5;
-            else reach = (int)(aq / charge_per_grid);
-            const int i0 = origin_w(xyz[3 * l]), j0 = origin_w(xyz[3 * l + 1]), k0 = origin_w(xyz[3 * l + 2]);
-            const float *ax = &dx[(size_t)l * ng1], *ay = &dy[(size_t)l * ng1], *az = &dz[(size_t)l * ng1];
-            for (int i = std::max(i0 - reach, 0); i < std::min(i0 + reach + 1, ng1); ++i)
-                for (int j = std::max(j0 - reach, 0); j < std::min(j0 + reach + 1, ng1); ++j) {
-                    const float d2 = ax[i] + ay[j];
-                    for (int k = std::max(k0 - reach, 0); k < std::min(k0 + reach + 1, ng1); ++k) {
-                        const size_t c = (size_t)ng2 * i + ng1 * j + k;
-                        if (grid_r[c] < 0.0) continue;   // receptor core
-                        const float r = std::sqrt(d2 + az[k]);
-                        float eps;
-                        if (r >= 8.0f) eps = 80.0f;
-                        else if (r > 6.0f) eps = 38.0f * r + -224.0f;
-                        else eps = 4.0f;
-                        grid_i[c] += e_ratio * beta * q / eps / r;
-                    }
-                }
+    receptor_electro(rec, p, gc, ng1, grid_r, nullptr, 1, grid_i.data());
+}
+
+void receptor_electro(const Molecule &rec, const Params &p, const std::vector<float> &gc, int ng1,
+                      const std::vector<float> &grid_r, const int *group, int ngroups, float *out) {
+    const int ng2 = ng1 * ng1;
+    const size_t ng3 = (size_t)ng2 * ng1;
+    const int na = rec.na();
+    const std::vector<float> xyz = centred_coordinates(rec);
+    std::fill(out, out + ng3 * ngroups, 0.0f);
+    std::vector<float> dx(ng1), dy(ng1), dz(ng1);
+    const float beta = -2800.0f;
+    const float e_ratio = p.elec_ratio;
+    const float width = gc[1] - gc[0];
+    const float charge_per_grid = -1 * width * 80.0f / (beta * e_ratio);
+    auto origin_w = [&](float c) { return (int)(c / width + ng1 / 2); };
+    for (int l = 0; l < na; ++l) {
+        const float q = rec.charge[l];
+        const float aq = std::fabs(q);
+        if (aq <= 1.0e-6f) continue;
+        const int g = group ? group[l] : 0;
+        if (g < 0 || g >= ngroups) continue;
+        float *grid_i = out + ng3 * g;
+        int reach;
+        if (aq < 0.07) reach = 4;
+        else if (aq < 0.21) reach = 5;
+        else reach = (int)(aq / charge_per_grid);
+        for (int c = 0; c < ng1; ++c) {
+            float a = xyz[3 * l] - gc[c], b = xyz[3 * l + 1] - gc[c], d = xyz[3 * l + 2] - gc[c];
+            dx[c] = a * a;
+            dy[c] = b * b;
+            dz[c] = d * d;
         }
+        const int i0 = origin_w(xyz[3 * l]), j0 = origin_w(xyz[3 * l + 1]), k0 = origin_w(xyz[3 * l + 2]);
+        for (int i = std::max(i0 - reach, 0); i < std::min(i0 + reach + 1, ng1); ++i)
+            for (int j = std::max(j0 - reach, 0); j < std::min(j0 + reach + 1, ng1); ++j) {
+                const float d2 = dx[i] + dy[j];
+                for (int k = std::max(k0 - reach, 0); k < std::min(k0 + reach + 1, ng1); ++k) {
+                    const size_t c = (size_t)ng2 * i + ng1 * j + k;
+                    if (grid_r[c] < 0.0) continue;   // receptor core
+                    const float r = std::sqrt(d2 + dz[k]);
+                    float eps;
+                    if (r >= 8.0f) eps = 80.0f;
+                    else if (r > 6.0f) eps = 38.0f * r + -224.0f;
+                    else eps = 4.0f;
+                    grid_i[c] += e_ratio * beta * q / eps / r;
+                }
+            }
     }
 }
 

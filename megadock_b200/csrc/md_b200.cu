@@ -737,16 +737,121 @@ int md_dock_pairs(md_ctx *runner, md_ctx *const *pairs, int npairs, const float 
     return MD_OK;
 }
 
+namespace {
+
+// Shared body of the adjoint entry points: per-pose rotation matrices (9 each),
+// translations and weights dL/ds on the host; host outputs (any may be null).
+int adjoint_core(md_ctx *ctx, const float *rotmat, int n, const int4 *shift, const float *w, float *d_rec_r,
+                 float *d_rec_i, float *d_charge, const int *lig_sel, int n_lig, float *d_lig_r, float *d_lig_i,
+                 float alpha, double *d_alpha) {
+    MD_CUDA(cudaSetDevice(ctx->device));
+    const int N = ctx->N, ng = ctx->ng;
+    const size_t ng3 = (size_t)ng * ng * ng;
+    const int B = std::max(1, std::min(ctx->batch, n));
+    int rc = ensure_work(ctx, B, 1);
+    if (rc) return rc;
+    float *d_rot = nullptr, *d_w = nullptr, *d_grad = nullptr, *d_vox = nullptr, *d_dq = nullptr, *d_lg = nullptr;
+    int4 *d_shift = nullptr;
+    int *d_sel = nullptr;
+    auto cleanup = [&]() {
+        cudaFree(d_rot);
+        cudaFree(d_w);
+        cudaFree(d_grad);
+        cudaFree(d_vox);
+        cudaFree(d_dq);
+        cudaFree(d_shift);
+        cudaFree(d_sel);
+        cudaFree(d_lg);
+    };
+    cudaError_t e = cudaSuccess;
+    auto step = [&](cudaError_t x) {
+        if (e == cudaSuccess) e = x;
+    };
+    step(cudaMalloc(&d_rot, sizeof(float) * 9 * n));
+    step(cudaMalloc(&d_w, sizeof(float) * n));
+    step(cudaMalloc(&d_shift, sizeof(int4) * n));
+    step(cudaMalloc(&d_grad, sizeof(float) * 2 * ng3));
+    step(cudaMalloc(&d_vox, sizeof(float) * 2 * ng3 * B));
+    step(cudaMalloc(&d_dq, sizeof(float) * std::max(ctx->na, 1)));
+    if (n_lig > 0) {
+        step(cudaMalloc(&d_sel, sizeof(int) * n_lig));
+        step(cudaMalloc(&d_lg, sizeof(float) * 2 * ng3 * n_lig));
+    }
+    cudaStream_t s = ctx->stream;
+    step(cudaMemcpyAsync(d_rot, rotmat, sizeof(float) * 9 * n, cudaMemcpyHostToDevice, s));
+    step(cudaMemcpyAsync(d_w, w, sizeof(float) * n, cudaMemcpyHostToDevice, s));
+    step(cudaMemcpyAsync(d_shift, shift, sizeof(int4) * n, cudaMemcpyHostToDevice, s));
+    step(cudaMemsetAsync(d_grad, 0, sizeof(float) * 2 * ng3, s));
+    if (e != cudaSuccess) {
+        ctx->err = std::string("adjoint: ") + cudaGetErrorString(e);
+        cleanup();
+        return MD_ERR_CUDA;
+    }
+    const int thr = 256;
+    const int blocks = (int)((ng3 + thr - 1) / thr);
+    // receptor gradient: voxel grids of each chunk of poses, then the gather
+    for (int r0 = 0; r0 < n; r0 += B) {
+        const int nb = std::min(B, n - r0);
+        launch_voxel_chunk(ctx, d_rot + 9 * (size_t)r0, nb, d_vox, d_vox + ng3 * B);
+        k_adj_receptor<<<blocks, thr, 0, s>>>(N, ng, nb, d_vox, d_vox + ng3 * B, d_shift + r0, d_w + r0, d_grad,
+                                              d_grad + ng3);
+    }
+    // charge gradient through the charge-cell assignment
+    GridView G{ng, ctx->gw, (float)(ng * ctx->gw) / 2, ctx->d_gc, ctx->d_tw};
+    LigandView L{ctx->na, ctx->d_atom, ctx->d_rad2, ctx->delta};
+    k_adj_charge<<<(ctx->na + 127) / 128, 128, 0, s>>>(L, G, N, n, d_rot, d_shift, d_w, ctx->d_recv + ng3, d_dq);
+    if (n_lig > 0) {
+        step(cudaMemcpyAsync(d_sel, lig_sel, sizeof(int) * n_lig, cudaMemcpyHostToDevice, s));
+        k_adj_ligand<<<dim3(blocks, n_lig), thr, 0, s>>>(N, ng, n_lig, d_sel, ctx->d_recv, ctx->d_recv + ng3,
+                                                         d_shift, d_w, d_lg, d_lg + ng3 * n_lig);
+    }
+    step(cudaGetLastError());
+    std::vector<float> gi(d_alpha ? ng3 : 0), ri(d_alpha ? ng3 : 0);
+    if (d_rec_r) step(cudaMemcpyAsync(d_rec_r, d_grad, sizeof(float) * ng3, cudaMemcpyDeviceToHost, s));
+    if (d_rec_i) step(cudaMemcpyAsync(d_rec_i, d_grad + ng3, sizeof(float) * ng3, cudaMemcpyDeviceToHost, s));
+    if (d_alpha) {
+        step(cudaMemcpyAsync(gi.data(), d_grad + ng3, sizeof(float) * ng3, cudaMemcpyDeviceToHost, s));
+        step(cudaMemcpyAsync(ri.data(), ctx->d_recv + ng3, sizeof(float) * ng3, cudaMemcpyDeviceToHost, s));
+    }
+    if (d_charge) step(cudaMemcpyAsync(d_charge, d_dq, sizeof(float) * ctx->na, cudaMemcpyDeviceToHost, s));
+    if (n_lig > 0) {
+        step(cudaMemcpyAsync(d_lig_r, d_lg, sizeof(float) * ng3 * n_lig, cudaMemcpyDeviceToHost, s));
+        step(cudaMemcpyAsync(d_lig_i, d_lg + ng3 * n_lig, sizeof(float) * ng3 * n_lig, cudaMemcpyDeviceToHost, s));
+    }
+    step(cudaStreamSynchronize(s));
+    cleanup();
+    if (e != cudaSuccess) {
+        ctx->err = std::string("adjoint: ") + cudaGetErrorString(e);
+        return MD_ERR_CUDA;
+    }
+    if (d_alpha) {
+        // the receptor's imaginary grid is alpha times a fixed-support unit grid
+        double acc = 0.0;
+        for (size_t x = 0; x < ng3; ++x) acc += (double)gi[x] * (double)ri[x];
+        *d_alpha = alpha != 0.f ? acc / alpha : std::nan("");
+    }
+    return MD_OK;
+}
+
+int check_lig_sel(md_ctx *ctx, int n, const int *lig_sel, int n_lig, const float *a, const float *b) {
+    if (n_lig < 0 || (n_lig > 0 && (!lig_sel || !a || !b))) return MD_ERR_ARG;
+    for (int m = 0; m < n_lig; ++m)
+        if (lig_sel[m] < 0 || lig_sel[m] >= n) {
+            ctx->err = "ligand-grid selection outside the pose list";
+            return MD_ERR_ARG;
+        }
+    return MD_OK;
+}
+
+}  // namespace
+
 int md_adjoint_lse(md_ctx *ctx, const float *rotmat, int n_rot, const md_pose *top1, float temperature, float alpha,
                    double *loss, float *d_rec_r, float *d_rec_i, float *d_charge, double *d_alpha,
                    const int *lig_rot, int n_lig_rot, float *d_lig_r, float *d_lig_i) {
     if (!ctx || !rotmat || !top1 || n_rot < 1 || !(temperature > 0.f)) return MD_ERR_ARG;
-    if (n_lig_rot > 0 && (!lig_rot || !d_lig_r || !d_lig_i)) return MD_ERR_ARG;
-    int rc = check_ready(ctx);
+    int rc = check_lig_sel(ctx, n_rot, lig_rot, n_lig_rot, d_lig_r, d_lig_i);
     if (rc) return rc;
-    MD_CUDA(cudaSetDevice(ctx->device));
-    const int N = ctx->N, ng = ctx->ng;
-    const size_t ng3 = (size_t)ng * ng * ng;
+    if ((rc = check_ready(ctx))) return rc;
     // loss and weights in double on the host: w_r = softmax(s_r / T); rotations
     // whose score was clamped to 0 (no positive cell) have no parameter gradient
     double smax = -1e300;
@@ -761,94 +866,80 @@ int md_adjoint_lse(md_ctx *ctx, const float *rotmat, int n_rot, const md_pose *t
         w[r] = live ? (float)(std::exp(((double)top1[r].score - smax) / temperature) / z) : 0.f;
         shift[r] = make_int4(top1[r].i, top1[r].j, top1[r].k, 0);
     }
-    const int B = std::max(1, std::min(ctx->batch, n_rot));
-    if ((rc = ensure_work(ctx, B, 1))) return rc;
-    // device scratch of this call
-    float *d_rot = nullptr, *d_w = nullptr, *d_grad = nullptr, *d_vox = nullptr, *d_dq = nullptr;
-    int4 *d_shift = nullptr;
-    auto cleanup = [&]() {
-        cudaFree(d_rot);
-        cudaFree(d_w);
-        cudaFree(d_grad);
-        cudaFree(d_vox);
-        cudaFree(d_dq);
-        cudaFree(d_shift);
-    };
-    auto fail = [&](cudaError_t e) {
-        ctx->err = std::string("adjoint: ") + cudaGetErrorString(e);
-        cleanup();
-        return MD_ERR_CUDA;
-    };
-    cudaError_t e = cudaSuccess;
-    if (e == cudaSuccess) e = cudaMalloc(&d_rot, sizeof(float) * 9 * n_rot);
-    if (e == cudaSuccess) e = cudaMalloc(&d_w, sizeof(float) * n_rot);
-    if (e == cudaSuccess) e = cudaMalloc(&d_shift, sizeof(int4) * n_rot);
-    if (e == cudaSuccess) e = cudaMalloc(&d_grad, sizeof(float) * 2 * ng3);
-    if (e == cudaSuccess) e = cudaMalloc(&d_vox, sizeof(float) * 2 * ng3 * B);
-    if (e == cudaSuccess) e = cudaMalloc(&d_dq, sizeof(float) * std::max(ctx->na, 1));
-    if (e != cudaSuccess) return fail(e);
-    cudaStream_t s = ctx->stream;
-    cudaMemcpyAsync(d_rot, rotmat, sizeof(float) * 9 * n_rot, cudaMemcpyHostToDevice, s);
-    cudaMemcpyAsync(d_w, w.data(), sizeof(float) * n_rot, cudaMemcpyHostToDevice, s);
-    cudaMemcpyAsync(d_shift, shift.data(), sizeof(int4) * n_rot, cudaMemcpyHostToDevice, s);
-    cudaMemsetAsync(d_grad, 0, sizeof(float) * 2 * ng3, s);
-    const int thr = 256;
-    const int blocks = (int)((ng3 + thr - 1) / thr);
-    // receptor gradient: voxel grids of each chunk of rotations, then the gather
-    for (int r0 = 0; r0 < n_rot; r0 += B) {
-        const int nb = std::min(B, n_rot - r0);
-        launch_voxel_chunk(ctx, d_rot + 9 * (size_t)r0, nb, d_vox, d_vox + ng3 * B);
-        k_adj_receptor<<<blocks, thr, 0, s>>>(N, ng, nb, d_vox, d_vox + ng3 * B, d_shift + r0, d_w + r0, d_grad,
-                                              d_grad + ng3);
-    }
-    // charge gradient through the charge-cell assignment
-    GridView G{ng, ctx->gw, (float)(ng * ctx->gw) / 2, ctx->d_gc, ctx->d_tw};
-    LigandView L{ctx->na, ctx->d_atom, ctx->d_rad2, ctx->delta};
-    k_adj_charge<<<(ctx->na + 127) / 128, 128, 0, s>>>(L, G, N, n_rot, d_rot, d_shift, d_w, ctx->d_recv + ng3, d_dq);
-    if ((e = cudaGetLastError()) != cudaSuccess) return fail(e);
-    std::vector<float> gr(ng3), gi(ng3);
-    if ((e = cudaMemcpyAsync(gr.data(), d_grad, sizeof(float) * ng3, cudaMemcpyDeviceToHost, s)) != cudaSuccess)
-        return fail(e);
-    if ((e = cudaMemcpyAsync(gi.data(), d_grad + ng3, sizeof(float) * ng3, cudaMemcpyDeviceToHost, s)) != cudaSuccess)
-        return fail(e);
-    if (d_charge &&
-        (e = cudaMemcpyAsync(d_charge, d_dq, sizeof(float) * ctx->na, cudaMemcpyDeviceToHost, s)) != cudaSuccess)
-        return fail(e);
-    // ligand-grid gradient of the selected rotations
-    if (n_lig_rot > 0) {
-        int *d_sel = nullptr;
-        float *d_lg = nullptr;
-        if ((e = cudaMalloc(&d_sel, sizeof(int) * n_lig_rot)) != cudaSuccess) return fail(e);
-        if ((e = cudaMalloc(&d_lg, sizeof(float) * 2 * ng3 * n_lig_rot)) != cudaSuccess) {
-            cudaFree(d_sel);
-            return fail(e);
+    return adjoint_core(ctx, rotmat, n_rot, shift.data(), w.data(), d_rec_r, d_rec_i, d_charge, lig_rot, n_lig_rot,
+                        d_lig_r, d_lig_i, alpha, d_alpha);
+}
+
+int md_adjoint_poses(md_ctx *ctx, const float *rotmat, int n, const md_pose *poses, const float *dl_ds,
+                     float *d_rec_r, float *d_rec_i, float *d_charge, const int *lig_pose, int n_lig,
+                     float *d_lig_r, float *d_lig_i) {
+    if (!ctx || !rotmat || !poses || !dl_ds || n < 1) return MD_ERR_ARG;
+    int rc = check_lig_sel(ctx, n, lig_pose, n_lig, d_lig_r, d_lig_i);
+    if (rc) return rc;
+    if ((rc = check_ready(ctx))) return rc;
+    std::vector<int4> shift(n);
+    for (int r = 0; r < n; ++r) {
+        if (poses[r].i < 0 || poses[r].i >= ctx->N || poses[r].j < 0 || poses[r].j >= ctx->N || poses[r].k < 0 ||
+            poses[r].k >= ctx->N) {
+            ctx->err = "pose translation outside [0, nf1)";
+            return MD_ERR_ARG;
         }
-        cudaMemcpyAsync(d_sel, lig_rot, sizeof(int) * n_lig_rot, cudaMemcpyHostToDevice, s);
-        k_adj_ligand<<<dim3(blocks, n_lig_rot), thr, 0, s>>>(N, ng, n_lig_rot, d_sel, ctx->d_recv, ctx->d_recv + ng3,
-                                                             d_shift, d_w, d_lg, d_lg + ng3 * n_lig_rot);
-        e = cudaMemcpyAsync(d_lig_r, d_lg, sizeof(float) * ng3 * n_lig_rot, cudaMemcpyDeviceToHost, s);
-        if (e == cudaSuccess)
-            e = cudaMemcpyAsync(d_lig_i, d_lg + ng3 * n_lig_rot, sizeof(float) * ng3 * n_lig_rot,
-                                cudaMemcpyDeviceToHost, s);
-        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-        cudaFree(d_sel);
-        cudaFree(d_lg);
-        if (e != cudaSuccess) return fail(e);
+        shift[r] = make_int4(poses[r].i, poses[r].j, poses[r].k, 0);
     }
-    if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return fail(e);
-    if (d_rec_r) std::copy(gr.begin(), gr.end(), d_rec_r);
-    if (d_rec_i) std::copy(gi.begin(), gi.end(), d_rec_i);
-    if (d_alpha) {
-        // the receptor's imaginary grid is alpha times a fixed-support unit grid
-        std::vector<float> ri(ng3);
-        if ((e = cudaMemcpy(ri.data(), ctx->d_recv + ng3, sizeof(float) * ng3, cudaMemcpyDeviceToHost)) !=
-            cudaSuccess)
-            return fail(e);
-        double acc = 0.0;
-        for (size_t x = 0; x < ng3; ++x) acc += (double)gi[x] * (double)ri[x];
-        *d_alpha = alpha != 0.f ? acc / alpha : std::nan("");
+    return adjoint_core(ctx, rotmat, n, shift.data(), dl_ds, d_rec_r, d_rec_i, d_charge, lig_pose, n_lig, d_lig_r,
+                        d_lig_i, 0.f, nullptr);
+}
+
+int md_pose_scores(md_ctx *ctx, const float *rotmat, int n, const md_pose *poses, float *scores) {
+    if (!ctx || !rotmat || !poses || !scores || n < 1) return MD_ERR_ARG;
+    int rc = check_ready(ctx);
+    if (rc) return rc;
+    MD_CUDA(cudaSetDevice(ctx->device));
+    const int N = ctx->N, ng = ctx->ng;
+    const size_t ng3 = (size_t)ng * ng * ng;
+    std::vector<int4> shift(n);
+    for (int r = 0; r < n; ++r) {
+        if (poses[r].i < 0 || poses[r].i >= N || poses[r].j < 0 || poses[r].j >= N || poses[r].k < 0 ||
+            poses[r].k >= N) {
+            ctx->err = "pose translation outside [0, nf1)";
+            return MD_ERR_ARG;
+        }
+        shift[r] = make_int4(poses[r].i, poses[r].j, poses[r].k, 0);
     }
-    cleanup();
+    const int B = std::max(1, std::min(ctx->batch, n));
+    if ((rc = ensure_work(ctx, B, 1))) return rc;
+    float *d_rot = nullptr, *d_vox = nullptr, *d_sc = nullptr;
+    int4 *d_shift = nullptr;
+    cudaError_t e = cudaSuccess;
+    auto step = [&](cudaError_t x) {
+        if (e == cudaSuccess) e = x;
+    };
+    step(cudaMalloc(&d_rot, sizeof(float) * 9 * n));
+    step(cudaMalloc(&d_shift, sizeof(int4) * n));
+    step(cudaMalloc(&d_sc, sizeof(float) * n));
+    step(cudaMalloc(&d_vox, sizeof(float) * 2 * ng3 * B));
+    cudaStream_t s = ctx->stream;
+    step(cudaMemcpyAsync(d_rot, rotmat, sizeof(float) * 9 * n, cudaMemcpyHostToDevice, s));
+    step(cudaMemcpyAsync(d_shift, shift.data(), sizeof(int4) * n, cudaMemcpyHostToDevice, s));
+    if (e == cudaSuccess) {
+        for (int r0 = 0; r0 < n; r0 += B) {
+            const int nb = std::min(B, n - r0);
+            launch_voxel_chunk(ctx, d_rot + 9 * (size_t)r0, nb, d_vox, d_vox + ng3 * B);
+            k_pose_dot<<<nb, 512, 0, s>>>(N, ng, ctx->d_recv, ctx->d_recv + ng3, d_vox, d_vox + ng3 * B,
+                                          d_shift + r0, d_sc + r0);
+        }
+        step(cudaGetLastError());
+        step(cudaMemcpyAsync(scores, d_sc, sizeof(float) * n, cudaMemcpyDeviceToHost, s));
+        step(cudaStreamSynchronize(s));
+    }
+    cudaFree(d_rot);
+    cudaFree(d_shift);
+    cudaFree(d_sc);
+    cudaFree(d_vox);
+    if (e != cudaSuccess) {
+        ctx->err = std::string("pose scores: ") + cudaGetErrorString(e);
+        return MD_ERR_CUDA;
+    }
     return MD_OK;
 }
 

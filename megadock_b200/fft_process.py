@@ -130,6 +130,41 @@ class FFTProcess:
                 "d_lig_r": dlr[:sel.size * ng3].reshape((sel.size,) + shape),
                 "d_lig_i": dli[:sel.size * ng3].reshape((sel.size,) + shape)}
 
+    def adjoint_poses(self, rotmats: np.ndarray, poses: np.ndarray, dl_ds: np.ndarray, lig_pose=()):
+        """Gradient for a loss with dL/d(score of pose p) = dl_ds[p]; pose p has
+        rotation matrix rotmats[p] and translation poses[p] i/j/k.  Returns a
+        dict: d_rec_r, d_rec_i (ng^3), d_charge (na), d_lig_r / d_lig_i for the
+        poses listed in lig_pose."""
+        m = np.ascontiguousarray(rotmats, dtype=np.float32).reshape(-1, 9)
+        poses = np.ascontiguousarray(poses).view(N.POSE_DTYPE).reshape(-1)
+        w = np.ascontiguousarray(dl_ds, dtype=np.float32).reshape(-1)
+        if not (len(m) == len(poses) == len(w)):
+            raise ValueError("one rotation matrix and one weight per pose")
+        ng3 = (self.num_fft // 2) ** 3
+        sel = np.ascontiguousarray(lig_pose, dtype=np.int32).reshape(-1)
+        drr = np.zeros(ng3, np.float32)
+        dri = np.zeros(ng3, np.float32)
+        dq = np.zeros(max(self._na, 1), np.float32)
+        dlr = np.zeros(max(sel.size, 1) * ng3, np.float32)
+        dli = np.zeros(max(sel.size, 1) * ng3, np.float32)
+        _check(N.lib().md_adjoint_poses(self._h, N.fptr(m), len(m), N.vptr(poses), N.fptr(w), N.fptr(drr),
+                                        N.fptr(dri), N.fptr(dq), sel.ctypes.data_as(C.POINTER(C.c_int)),
+                                        int(sel.size), N.fptr(dlr), N.fptr(dli)), self._h)
+        shape = ((self.num_fft // 2),) * 3
+        return {"d_rec_r": drr.reshape(shape), "d_rec_i": dri.reshape(shape), "d_charge": dq[:self._na],
+                "d_lig_r": dlr[:sel.size * ng3].reshape((sel.size,) + shape),
+                "d_lig_i": dli[:sel.size * ng3].reshape((sel.size,) + shape)}
+
+    def pose_scores(self, rotmats: np.ndarray, poses: np.ndarray) -> np.ndarray:
+        """Scores of given poses (rotation matrix per pose, translation i/j/k)."""
+        m = np.ascontiguousarray(rotmats, dtype=np.float32).reshape(-1, 9)
+        poses = np.ascontiguousarray(poses).view(N.POSE_DTYPE).reshape(-1)
+        if len(m) != len(poses):
+            raise ValueError("one rotation matrix per pose")
+        out = np.zeros(len(m), np.float32)
+        _check(N.lib().md_pose_scores(self._h, N.fptr(m), len(m), N.vptr(poses), N.fptr(out)), self._h)
+        return out
+
     # -- FFTProcess::sort_index / top_score / top_index
     def sort_index(self, nout: int):
         self._top = N.sort_poses(self._top, nout)
@@ -191,6 +226,19 @@ class Job:
         i = np.zeros(n, np.float32)
         N.lib().md_job_receptor_grids(self._h, N.fptr(r), N.fptr(i))
         return r.reshape((self.ng1,) * 3), i.reshape((self.ng1,) * 3)
+
+    def receptor_elec_groups(self, group, ngroups: int) -> np.ndarray:
+        """The receptor's electrostatic grid split by atom group (ngroups grids
+        of ng1^3; atom l goes to group[l], negative = left out)."""
+        g = np.ascontiguousarray(group, dtype=np.int32)
+        if len(g) != self.na_rec:
+            raise ValueError("one group per receptor atom")
+        out = np.zeros((ngroups,) + (self.ng1,) * 3, np.float32)
+        rc = N.lib().md_job_receptor_elec_groups(self._h, g.ctypes.data_as(C.POINTER(C.c_int)), int(ngroups),
+                                                 N.fptr(out))
+        if rc:
+            raise MdError(rc, "md_job_receptor_elec_groups")
+        return out
 
     def ligand_atoms(self):
         xyz = np.zeros(3 * self.na_lig, np.float32)

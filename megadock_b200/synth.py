@@ -220,3 +220,93 @@ def uneven_pairs(npairs=64, seed_base=2000, lo=60, hi=800):
         a, b = np.exp(rng.uniform(math.log(lo), math.log(hi), size=2))
         out.append((int(round(max(a, b))), int(round(min(a, b))), seed_base + p))
     return out
+
+
+# ---------------------------------------------------------------------------
+# Planted complexes for fitting: a ligand rigidly placed in contact with the
+# receptor surface, written in a rotated frame so that one rotation of the
+# docking set and one grid translation restore the native placement exactly.
+
+@dataclass
+class PlantedComplex:
+    rec_pdb: str
+    lig_pdb: str
+    rot_index: int             # rotation of the set that restores the native orientation
+    shift: np.ndarray          # native translation in grid cells (signed)
+    native_ca: np.ndarray      # native ligand C-alpha coordinates (receptor file frame)
+    lig_file_ca: np.ndarray    # ligand C-alpha coordinates as written in the ligand file
+    lig_ca_index: np.ndarray   # positions of the C-alphas in the ligand's heavy-atom list
+
+
+def _bbox_mid(xyz):
+    return (xyz.min(0) + xyz.max(0)) / 2
+
+
+def _rounded(xyz):
+    return np.round(np.asarray(xyz, np.float64), 3)
+
+
+def decoy_ca(lig_file_ca, lig_center, rec_center, rotmat9, shift_signed, grid_width):
+    """Ligand C-alphas of a docking pose: R (x - lig_center) - t * gw +
+    rec_center, the placement a pose (rotation, translation t, t >= N/2 read
+    as t - N) encodes (the score at t pairs receptor cell x with ligand cell
+    x + t; both grids are centred on their molecule's bounding-box centre)."""
+    m = np.asarray(rotmat9, np.float64).reshape(3, 3)
+    return (np.asarray(lig_file_ca, np.float64) - lig_center) @ m.T - np.asarray(shift_signed) * grid_width + rec_center
+
+
+def plant_complex(outdir, n_rec: int, n_lig: int, seed: int, rotation_set: int = 3600, grid_width: float = 1.2,
+                  contact: float = 4.0, stem: str | None = None) -> PlantedComplex:
+    """Receptor and ligand chains from `seed`; the ligand is moved along a
+    seeded direction from the receptor centre until its closest heavy atom is
+    `contact` A from the receptor (the native placement), then written
+    rotated by the transpose of a seeded rotation of the docking set."""
+    from scipy.spatial import cKDTree
+
+    from ._native import data_dir, rotation_matrix
+    os.makedirs(outdir, exist_ok=True)
+    stem = stem or f"pl{seed}"
+    rec, lig = make_pair(n_rec, n_lig, seed)
+    rng = np.random.default_rng(np.random.SeedSequence(seed).spawn(3)[2])
+    rec_xyz = np.array([a[3] for a in rec.atoms])
+    lig_xyz = np.array([a[3] for a in lig.atoms])
+    lig_xyz = lig_xyz - lig_xyz.mean(0)
+    tree = cKDTree(rec_xyz)
+    u = _random_unit(rng)
+    centre = rec_xyz.mean(0)
+    lo, hi = 0.0, 400.0                      # distance along u: overlap at lo, apart at hi
+    for _ in range(60):
+        mid = (lo + hi) / 2
+        d, _ = tree.query(lig_xyz + centre + mid * u)
+        if d.min() < contact:
+            lo = mid
+        else:
+            hi = mid
+    native = lig_xyz + centre + hi * u
+    angles = np.fromfile(os.path.join(data_dir(), f"rotations_{rotation_set}.f32"), np.float32).reshape(-1, 3)
+    k = int(rng.integers(len(angles)))
+    m = rotation_matrix(angles[k]).astype(np.float64).reshape(3, 3)
+    file_xyz = _rounded((native - native.mean(0)) @ m + np.array([40.0, 20.0, -12.0]))
+    rec_file = _rounded(rec_xyz)
+    rec_c = _bbox_mid(rec_file.astype(np.float32).astype(np.float64))
+    lig_c = _bbox_mid(file_xyz.astype(np.float32).astype(np.float64))
+    ca = np.array([i for i, a in enumerate(lig.atoms) if a[0] == "CA"])
+    placed = decoy_ca(file_xyz, lig_c, rec_c, m.reshape(-1), np.zeros(3), grid_width)
+    shift = np.round((placed - native).mean(0) / grid_width).astype(np.int64)
+    native_ca = decoy_ca(file_xyz[ca], lig_c, rec_c, m.reshape(-1), shift, grid_width)
+    rp = os.path.join(outdir, f"{stem}_r.pdb")
+    lp = os.path.join(outdir, f"{stem}_l.pdb")
+    write_pdb(rp, Chain(rec.resnames, [(a[0], a[1], a[2], x) for a, x in zip(rec.atoms, rec_file)]), "A")
+    write_pdb(lp, Chain(lig.resnames, [(a[0], a[1], a[2], x) for a, x in zip(lig.atoms, file_xyz)]), "B")
+    return PlantedComplex(rp, lp, k, shift, native_ca, file_xyz[ca], ca)
+
+
+def fitting_pairs(npairs=32, seed_base=4000, lo=200, hi=1500):
+    """(n_rec, n_lig, seed) of the fitting workload: chain lengths log-uniform
+    in [lo, hi] residues, seed = seed_base + pair index."""
+    rng = np.random.default_rng(seed_base)
+    out = []
+    for p in range(npairs):
+        n_rec, n_lig = np.exp(rng.uniform(np.log(lo), np.log(hi), 2)).astype(int)
+        out.append((int(n_rec), int(n_lig), seed_base + p))
+    return out

@@ -76,25 +76,30 @@ def weights(scores, temperature: float):
 
 
 class NumpyFFT:
-    """FP64 FFTs on the host."""
+    """FP64 FFTs on the host.  Grids are ng^3, embedded at offset N/4 of the
+    N^3 box; correlate(A, B)(t) = sum_x Re(conj(a(x)) b(x + t)) from the
+    spectra A, B of a and b."""
+
+    def spectrum(self, re, im=None):
+        z = O.embed(re, np.zeros_like(re) if im is None else im, self.N)
+        return np.fft.fftn(z)
+
+    def correlate(self, A, B):
+        return np.fft.ifftn(np.conj(A) * B).real
 
     def grids(self, rec_r, rec_i, N):
         self.N = N
-        self.Rc = np.conj(np.fft.fftn(O.embed(rec_r, rec_i, N)))
-        self.Ri = np.conj(np.fft.fftn(O.embed(np.zeros_like(rec_i), rec_i, N).imag))
+        self.R = self.spectrum(rec_r, rec_i)
+        self.Ri = self.spectrum(rec_i)
 
     def scores(self, lig_r, lig_i):
-        """(S, E): the score grid (the correlation, i.e. the unnormalised
-        inverse FFT divided by N^3) and its electrostatic part, float64 N^3."""
-        N = self.N
-        L = np.fft.fftn(O.embed(lig_r, lig_i, N))
-        Li = np.fft.fftn(O.embed(np.zeros_like(lig_i), lig_i, N).imag)
-        S = np.fft.ifftn(self.Rc * L).real
-        E = np.fft.ifftn(self.Ri * Li).real
-        return S, E
+        """(S, E, L): the score grid (the unnormalised inverse FFT divided by
+        N^3), its electrostatic part and the ligand spectrum, float64."""
+        L = self.spectrum(lig_r, lig_i)
+        return self.correlate(self.R, L), self.correlate(self.Ri, self.spectrum(lig_i)), L
 
 
-class TorchFFT:
+class TorchFFT(NumpyFFT):
     """FP64 FFTs on a CUDA device through torch (a checker only)."""
 
     def __init__(self, device="cuda:0"):
@@ -110,18 +115,13 @@ class TorchFFT:
         z[off:off + ng, off:off + ng, off:off + ng] = torch.from_numpy(np.asarray(g, np.float64)).to(self.dev)
         return z
 
-    def grids(self, rec_r, rec_i, N):
+    def spectrum(self, re, im=None):
         torch = self.torch
-        self.N = N
-        self.Rc = torch.conj(torch.fft.fftn(torch.complex(self._embed(rec_r), self._embed(rec_i))))
-        self.Ri = torch.conj(torch.fft.fftn(self._embed(rec_i)))
+        z = self._embed(re) if im is None else torch.complex(self._embed(re), self._embed(im))
+        return torch.fft.fftn(z)
 
-    def scores(self, lig_r, lig_i):
-        torch = self.torch
-        Lr, Li = self._embed(lig_r), self._embed(lig_i)
-        S = torch.fft.ifftn(self.Rc * torch.fft.fftn(torch.complex(Lr, Li))).real
-        E = torch.fft.ifftn(self.Ri * torch.fft.fftn(Li)).real
-        return S, E
+    def correlate(self, A, B):
+        return self.torch.fft.ifftn(self.torch.conj(A) * B).real
 
 
 def _gather(G, part, ijk, t, N):
@@ -132,6 +132,17 @@ def _gather(G, part, ijk, t, N):
     out = np.zeros(len(ijk))
     out[ok] = G[part[ok], idx[0][ok], idx[1][ok], idx[2][ok]]
     return out
+
+
+def _to_np(a):
+    return a if isinstance(a, np.ndarray) else a.cpu().numpy()
+
+
+def _take(grid, idx):
+    if isinstance(grid, np.ndarray):
+        return grid.reshape(-1)[idx]
+    import torch
+    return grid.reshape(-1)[torch.from_numpy(idx).to(grid.device)].cpu().numpy()
 
 
 def _candidates(S, E, h, coef_max, alpha):
@@ -169,14 +180,18 @@ class Coordinates:
     1 imaginary, flat ng^3 index), ligand atoms (charges), ligand cells of
     selected rotations (rotation index, part, flat index) and alpha."""
 
-    def __init__(self, rec=(), atoms=(), lig=(), alpha=False):
+    def __init__(self, rec=(), atoms=(), lig=(), alpha=False, dirs=()):
         self.rec = [(int(p), int(x)) for p, x in rec]
         self.atoms = [int(a) for a in atoms]
         self.lig = [(int(r), int(p), int(y)) for r, p, y in lig]
         self.alpha = bool(alpha)
+        # directions in parameter space: dict(rec_r=grid, rec_i=grid, atoms=vector),
+        # any key optional; the coordinate moves the receptor grids by h * rec_*
+        # and the ligand charges by h * atoms
+        self.dirs = list(dirs)
 
     def __len__(self):
-        return len(self.rec) + len(self.atoms) + len(self.lig) + int(self.alpha)
+        return len(self.rec) + len(self.atoms) + len(self.lig) + len(self.dirs) + int(self.alpha)
 
 
 class AdjointReference:
@@ -208,14 +223,19 @@ class AdjointReference:
         return xr, gr, gi
 
     def run(self, rotmats, shifts, scores, temperature, alpha, lig_rot=(), coords: Coordinates | None = None,
-            h=1e-3, check_cells=True):
+            h=1e-3, check_cells=True, dl_ds=None, fixed=None):
         """rotmats (n, 9); shifts (n, 3) and scores (n,) are the translations and
-        top-1 scores the gradient is taken at (e.g. the device's).  Returns the
-        reference gradient (dict) and, with coords, the finite-difference
-        tables."""
+        top-1 scores the gradient is taken at (e.g. the device's).  dl_ds
+        replaces the log-sum-exp weights by given ones; fixed[n] marks entries
+        whose score is the value at the given translation (not a maximum over
+        translations, not clamped at 0).  Returns the reference gradient (dict)
+        and, with coords, the finite-difference tables."""
         ng, N = self.ng, self.N
         n = len(rotmats)
         loss, w = weights(scores, temperature)
+        if dl_ds is not None:
+            loss, w = None, np.asarray(dl_ds, np.float64)
+        fixed = np.zeros(n, bool) if fixed is None else np.asarray(fixed, bool)
         dRr = np.zeros((ng,) * 3)
         dRi = np.zeros((ng,) * 3)
         dq = np.zeros(len(self.charge))
@@ -233,6 +253,8 @@ class AdjointReference:
             rec_x = np.array([x for _, x in coords.rec], np.int64).reshape(-1)
             rec_ijk = np.stack([rec_x // (ng * ng), (rec_x // ng) % ng, rec_x % ng], -1)
             atoms = np.array(coords.atoms, np.int64)
+            nlig = len(coords.lig)
+            dir_spec = {}
         for r in range(n):
             xr, gr, gi = self.ligand(rotmats[r])
             cells = charge_cells(xr, ng, self.gw)
@@ -258,9 +280,32 @@ class AdjointReference:
                          w[r] * shifted(self.rec_i.astype(np.float64), N, minus))
             if coords is None:
                 continue
-            S, E = self.fft.scores(gr, gi)
+            S, E, Lspec = self.fft.scores(gr, gi)
             lig_max = max(float(np.abs(gr).max()), float(np.abs(gi).max()), self.max_rec)
-            top, am, cand, Sc, Ec = _candidates(S, E, h, lig_max, alpha if coords.alpha else None)
+            dgrids = []
+            for k, d in enumerate(coords.dirs):            # dS(t)/d(direction): full grids
+                g = None
+                if d.get("rec_r") is not None or d.get("rec_i") is not None:
+                    if k not in dir_spec:
+                        z = np.zeros((ng,) * 3)
+                        dir_spec[k] = self.fft.spectrum(d.get("rec_r", z) if d.get("rec_r") is not None else z,
+                                                        d.get("rec_i", z) if d.get("rec_i") is not None else z)
+                    g = self.fft.correlate(dir_spec[k], Lspec)
+                if d.get("atoms") is not None:
+                    Q = np.zeros((ng,) * 3)
+                    np.add.at(Q, (cells[:, 0], cells[:, 1], cells[:, 2]), np.asarray(d["atoms"], np.float64))
+                    ga = self.fft.correlate(self.fft.Ri, self.fft.spectrum(Q))
+                    g = ga if g is None else g + ga
+                dgrids.append(g)
+                lig_max = max(lig_max, float(abs(g).max()))
+            if fixed[r]:
+                am = int((t[0] * N + t[1]) * N + t[2])
+                cand = np.array([am], np.int64)
+                Sc = _to_np(S.reshape(-1)[am:am + 1]).astype(np.float64)
+                Ec = _to_np(E.reshape(-1)[am:am + 1]).astype(np.float64)
+                top = float(Sc[0])
+            else:
+                top, am, cand, Sc, Ec = _candidates(S, E, h, lig_max, alpha if coords.alpha else None)
             top64[r] = top
             arg64[r] = _ijk(am, N)
             tc = _ijk(cand, N)
@@ -279,6 +324,8 @@ class AdjointReference:
                     ys = np.array([y for _, _, y in rows], np.int64)
                     yijk = np.stack([ys // (ng * ng), (ys // ng) % ng, ys % ng], -1)
                     coef[nrec + nat + ks, c] = _gather(self.rec2, ps, yijk, -tc[c], N)
+            for k, g in enumerate(dgrids):
+                coef[nrec + nat + nlig + k] = _take(g, cand)
             if coords.alpha:                               # dS(t)/dalpha = E(t) / alpha
                 coef[-1] = Ec / alpha
             cand_S.append(Sc)
@@ -289,26 +336,31 @@ class AdjointReference:
                "d_lig": dL}
         if coords is not None:
             out["fd"] = FiniteDifferences(np.concatenate(cand_S), np.concatenate(cand_coef, axis=1),
-                                          np.array(seg[:-1]), top64, arg64)
+                                          np.array(seg[:-1]), top64, arg64, ~fixed)
         return out
 
 
 class FiniteDifferences:
     """Central differences of the FP64 loss from the candidate tables."""
 
-    def __init__(self, S, coef, starts, top, arg):
+    def __init__(self, S, coef, starts, top, arg, clamp):
         self.S, self.coef, self.starts = S, coef, starts
         self.top, self.arg = top, arg
+        self.clamp = clamp
 
-    def losses(self, rot_mask, k, step, temperature):
+    def _floor(self, s):
+        return np.where(self.clamp, np.maximum(s, 0.0), s)
+
+    def losses(self, rot_mask, k, step, temperature, loss_fn=None):
         """(loss, loss with every maximiser held at the unperturbed one) after
         moving coordinate k by step."""
+        f = loss_fn or (lambda s: _lse(s, temperature))
         v = self.S + step * self.coef[k]
-        s = np.maximum(np.maximum.reduceat(v, self.starts), 0.0)[rot_mask]
-        lin = np.maximum(v[self.starts], 0.0)[rot_mask]
-        return _lse(s, temperature), _lse(lin, temperature)
+        s = self._floor(np.maximum.reduceat(v, self.starts))[rot_mask]
+        lin = self._floor(v[self.starts])[rot_mask]
+        return f(s), f(lin)
 
-    def gradient(self, rot_mask, h, temperature, switch_tol=1e-4):
+    def gradient(self, rot_mask, h, temperature, switch_tol=1e-4, loss_fn=None):
         """(fd, differentiable): per coordinate the central difference and
         whether it moves by at most switch_tol (relative) when every rotation's
         maximiser is held fixed, i.e. whether changes of maximiser within +-h
@@ -317,8 +369,8 @@ class FiniteDifferences:
         fd = np.zeros(nk)
         ok = np.zeros(nk, bool)
         for k in range(nk):
-            lp, lp_lin = self.losses(rot_mask, k, h, temperature)
-            lm, lm_lin = self.losses(rot_mask, k, -h, temperature)
+            lp, lp_lin = self.losses(rot_mask, k, h, temperature, loss_fn)
+            lm, lm_lin = self.losses(rot_mask, k, -h, temperature, loss_fn)
             fd[k] = (lp - lm) / (2 * h)
             fd_lin = (lp_lin - lm_lin) / (2 * h)
             ok[k] = abs(fd[k] - fd_lin) <= switch_tol * abs(fd[k])

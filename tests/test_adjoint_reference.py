@@ -20,7 +20,7 @@ def _problem(pairs, n_rot=48):
     scores = np.zeros(n_rot)
     for r in range(n_rot):
         _, gr, gi = ref.ligand(rots[r])
-        S, _ = ref.fft.scores(gr, gi)
+        S, _, _ = ref.fft.scores(gr, gi)
         S = S.reshape(-1)
         am = int(np.argmax(S))
         shifts[r] = (am // job.nf1 ** 2, (am // job.nf1) % job.nf1, am % job.nf1)
@@ -73,3 +73,45 @@ def test_weights_clamped_rotations():
     loss, w = A.weights([0.0, 10.0, 20.0], 10.0)
     assert w[0] == 0.0 and w[2] > w[1] > 0
     assert np.isclose(loss, 20 + 10 * np.log(np.exp(-2) + np.exp(-1) + 1))
+
+
+def test_directions_and_fixed_entries(built, pairs):
+    """Directions reproduce the single-coordinate differences (alpha as the
+    receptor direction Ri / alpha, a charge as a unit atom vector), and a
+    ranking loss over a fixed-translation entry plus maxima matches its
+    analytic gradient through dl_ds."""
+    from oracle import adjoint as A
+    job, ref, rots, shifts, scores = _problem(pairs, n_rot=24)
+    T, alpha = 10.0, 1.0
+    a0 = 3
+    unit = np.zeros(len(ref.charge))
+    unit[a0] = 1.0
+    dirs = [dict(rec_i=ref.rec_i / alpha), dict(atoms=unit),
+            dict(rec_r=np.ones_like(ref.rec_r), rec_i=ref.rec_i, atoms=ref.charge.astype(np.float64))]
+    # entry 0: rotation 5 at a translation one cell away from its maximiser, held fixed
+    rots2 = np.concatenate([rots[5:6], rots])
+    sh2 = np.concatenate([(shifts[5:6] + [0, 0, 1]) % job.nf1, shifts])
+    fixed = np.zeros(len(rots2), bool)
+    fixed[0] = True
+    coords = A.Coordinates(atoms=[a0], alpha=True, dirs=dirs)
+    out0 = ref.run(rots2, sh2, np.concatenate([[1.0], scores]), T, alpha, coords=coords, fixed=fixed,
+                   dl_ds=np.zeros(len(rots2)), check_cells=False)
+    fdt = out0["fd"]
+    s = fdt.S[fdt.starts]
+    s = np.where(fixed, s, np.maximum(s, 0))
+    m = s.max()
+    p = np.exp((s - m) / T)
+    p /= p.sum()
+    w = p.copy()
+    w[0] -= 1.0
+    w[~fixed & (s <= 0)] = 0.0
+    loss_fn = lambda v: -v[0] + A._lse(v, T)
+    g = ref.run(rots2, sh2, s, T, alpha, dl_ds=w, fixed=fixed, check_cells=False)
+    fd, ok = fdt.gradient(np.ones(len(rots2), bool), 1e-3, T, loss_fn=loss_fn)
+    assert ok.all()
+    # rows: atom a0, dir alpha, dir unit atom, dir mixed, alpha
+    an_atom = g["d_charge"][a0]
+    an_alpha = g["d_alpha"]
+    an_mixed = g["d_rec_r"].sum() + (g["d_rec_i"] * ref.rec_i).sum() + g["d_charge"] @ ref.charge
+    want = np.array([an_atom, an_alpha, an_atom, an_mixed, an_alpha])
+    assert np.allclose(fd, want, rtol=1e-6, atol=1e-9 * np.abs(want).max()), (fd, want)
