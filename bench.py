@@ -222,6 +222,125 @@ def run_pairs_workload(args):
     print(json.dumps(line, default=float))
 
 
+def _timed_wall(fn, steps, warmup):
+    import torch
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        fn()
+    torch.cuda.synchronize()
+    return 1000.0 * (time.perf_counter() - t0) / steps
+
+
+def run_adjoint_workload(args):
+    """The 150/70-residue pair at N = 96, 3,600 rotations: one step = the
+    batched forward (t = 1, device-resident rotations and poses) plus the
+    adjoint of T * log(sum_r exp(s_r / T)) at T = 10 through the C ABI (top-1
+    poses in, receptor / charge / alpha gradients out)."""
+    import numpy as np
+    import torch
+
+    from megadock_b200 import FFTProcess, Job, POSE_DTYPE, rotation_matrices, synth
+    torch.cuda.set_device(0)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    with tempfile.TemporaryDirectory() as tmp:
+        rp, lp = synth.write_pair(tmp, 150, 70, 0, stem="adj")
+        job = Job(["-R", rp, "-L", lp, "-F", "96", "-r", "3600"])
+        rr, ri = job.receptor_grids()
+        xyz, rad, q = job.ligand_atoms()
+    mats = rotation_matrices(job.rotation_angles())
+    n = len(mats)
+    fp = FFTProcess(0, stream=stream.cuda_stream)
+    fp.alloc_array(job.nf1, job.grid_width, job.grid_coord())
+    fp.receptor_fft(rr, ri)
+    fp.ligand_data_transfer_gpu(xyz, rad, q, job.lig_core)
+    fp.set_batch(args.batch or 64)
+    d_rot = torch.from_numpy(mats).cuda()
+    d_pose = torch.zeros(n * 5, dtype=torch.int32, device="cuda")
+    state = {}
+
+    def fwd():
+        fp.dock_device(d_rot.data_ptr(), 0, n, 1, d_pose.data_ptr())
+
+    def step():
+        fwd()
+        top1 = d_pose.cpu().numpy().view(POSE_DTYPE)
+        state["res"] = fp.adjoint_lse(mats, top1, 10.0, 1.0)
+        state["live"] = int((top1["score"] > 0).sum())
+
+    with Clocks(0) as clk:
+        ms = _timed_wall(step, args.steps, args.warmup)
+    ms_fwd = _timed_wall(fwd, args.steps, 1)
+    top1 = d_pose.cpu().numpy().view(POSE_DTYPE)
+    s = top1["score"].astype(np.float64)
+    w = np.exp((s - s.max()) / 10.0)
+    w /= w.sum()
+    nz = int((w.astype(np.float32) != 0).sum())
+    line = {
+        "metric": "rotations/sec, forward + adjoint of LSE(T=10) over per-rotation top-1 scores, 96^3, 3,600 rot",
+        "value": n / (ms * 1e-3), "unit": "rotations/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": f"adjoint, 150/70-residue synthetic pair ({job.na_rec}/{job.na_lig} atoms), N=96, "
+                               f"3600 rotations, t=1, T=10", "timing": "wall clock around synchronous C-ABI calls"},
+        "forward_ms": ms_fwd, "adjoint_ms": ms - ms_fwd, "rotations_with_weight": nz,
+        "loss": state["res"]["loss"], "d_alpha": state["res"]["d_alpha"],
+        "clocks": clk.summary(),
+    }
+    fp.fft_memory_free()
+    print(json.dumps(line, default=float))
+
+
+def run_fit_workload(args):
+    """32 planted complexes (chains log-uniform in 200-1,500 residues), the
+    54,000-rotation set, N chosen per pair: one step = the forward (batched,
+    t = 1) and the ranking-loss adjoint of every pair at the current alpha and
+    charge scales, i.e. one gradient evaluation of the fit."""
+    import collections
+
+    import torch
+
+    from megadock_b200 import synth
+    from megadock_b200.fit import Fitter, FitPair
+    from megadock_b200.pairs import choose_fft_size
+    torch.cuda.set_device(0)
+    t_setup = time.perf_counter()
+    tmp = tempfile.mkdtemp(prefix="md_fit_")
+    pairs = []
+    for nr, nl, seed in synth.fitting_pairs(args.fit_pairs):
+        pc = synth.plant_complex(tmp, nr, nl, seed, rotation_set=54000)
+        pairs.append(FitPair(pc, choose_fft_size(pc.rec_pdb, pc.lig_pdb), 54000, batch=args.batch or 64))
+    t_setup = time.perf_counter() - t_setup
+    f = Fitter(pairs, alpha=1.0, temperature=10.0)
+    state = {}
+
+    def step():
+        state["eval"] = f.evaluate()
+
+    with Clocks(0) as clk:
+        ms = _timed_wall(step, args.steps, args.warmup)
+    loss, ga, gs, stats = state["eval"]
+    evals = sum(len(p.mats) for p in pairs)
+    sizes = collections.Counter(p.N for p in pairs)
+    line = {
+        "metric": "pair-evaluations/sec, forward + ranking-loss adjoint, 32 planted pairs, 54,000 rotations each",
+        "value": evals / (ms * 1e-3), "unit": "rotation-evaluations/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"{len(pairs)} planted complexes, chains log-uniform 200-1500 residues, "
+                               "54000 rotations, t=1, T=10, negatives > 10 A C-alpha RMSD",
+                   "fft_sizes": {str(k): v for k, v in sorted(sizes.items())},
+                   "timing": "wall clock around synchronous C-ABI calls, host label and chain-rule work included"},
+        "loss": loss, "d_alpha": ga, "adjoint_poses": int(sum(st["n_adj"] for st in stats)),
+        "positive_rank_median": float(statistics.median(st["rank"] for st in stats)),
+        "setup_s": t_setup, "clocks": clk.summary(),
+    }
+    print(json.dumps(line, default=float))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -230,8 +349,11 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--batch", type=int, default=0, help="rotations per launch (0 = autotune)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="metric", choices=["metric", "pairs"],
-                    help="metric: the headline workload; pairs: 64 uneven synthetic pairs, 3,600 rotations each")
+    ap.add_argument("--workload", default="metric", choices=["metric", "pairs", "adjoint", "fit"],
+                    help="metric: the headline workload; pairs: 64 uneven synthetic pairs, 3,600 rotations each; "
+                         "adjoint: forward + LSE adjoint at 96^3, 3,600 rotations; fit: one ranking-loss gradient "
+                         "evaluation over 32 planted pairs, 54,000 rotations each")
+    ap.add_argument("--fit-pairs", type=int, default=32)
     ap.add_argument("--profile-case", type=int, default=0, metavar="R",
                     help="run R rotations of the batched form once (for ncu captures) and exit")
     args = ap.parse_args()
@@ -241,6 +363,10 @@ def main():
         return run_profile_case(args)
     if args.workload == "pairs":
         return run_pairs_workload(args)
+    if args.workload == "adjoint":
+        return run_adjoint_workload(args)
+    if args.workload == "fit":
+        return run_fit_workload(args)
 
     import numpy as np
     import torch

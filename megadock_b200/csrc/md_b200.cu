@@ -866,7 +866,35 @@ int md_adjoint_lse(md_ctx *ctx, const float *rotmat, int n_rot, const md_pose *t
         w[r] = live ? (float)(std::exp(((double)top1[r].score - smax) / temperature) / z) : 0.f;
         shift[r] = make_int4(top1[r].i, top1[r].j, top1[r].k, 0);
     }
-    return adjoint_core(ctx, rotmat, n_rot, shift.data(), w.data(), d_rec_r, d_rec_i, d_charge, lig_rot, n_lig_rot,
+    // only rotations with a nonzero float weight (or a requested ligand grid)
+    // contribute: compact them, keeping their order
+    std::vector<int> idx, remap(n_rot, -1);
+    std::vector<char> want(n_rot, 0);
+    for (int m = 0; m < n_lig_rot; ++m) want[lig_rot[m]] = 1;
+    for (int r = 0; r < n_rot; ++r)
+        if (w[r] != 0.f || want[r]) {
+            remap[r] = (int)idx.size();
+            idx.push_back(r);
+        }
+    if (idx.empty()) {   // no live rotation: every gradient is zero
+        const size_t ng3 = (size_t)ctx->ng * ctx->ng * ctx->ng;
+        if (d_rec_r) std::fill(d_rec_r, d_rec_r + ng3, 0.f);
+        if (d_rec_i) std::fill(d_rec_i, d_rec_i + ng3, 0.f);
+        if (d_charge) std::fill(d_charge, d_charge + ctx->na, 0.f);
+        if (d_alpha) *d_alpha = 0.0;
+        return MD_OK;
+    }
+    const int nc = (int)idx.size();
+    std::vector<float> mc(9 * (size_t)nc), wc(nc);
+    std::vector<int4> sc(nc);
+    for (int c = 0; c < nc; ++c) {
+        std::copy(rotmat + 9 * (size_t)idx[c], rotmat + 9 * (size_t)idx[c] + 9, mc.begin() + 9 * (size_t)c);
+        wc[c] = w[idx[c]];
+        sc[c] = shift[idx[c]];
+    }
+    std::vector<int> lc(n_lig_rot);
+    for (int m = 0; m < n_lig_rot; ++m) lc[m] = remap[lig_rot[m]];
+    return adjoint_core(ctx, mc.data(), nc, sc.data(), wc.data(), d_rec_r, d_rec_i, d_charge, lc.data(), n_lig_rot,
                         d_lig_r, d_lig_i, alpha, d_alpha);
 }
 

@@ -47,13 +47,24 @@ def residue_codes(pdb_path) -> np.ndarray:
 def pose_rmsd(poses, mats, lig_file_ca, lig_center, rec_center, native_ca, nfft, grid_width) -> np.ndarray:
     """Ligand C-alpha RMSD to native_ca of each pose (rotation index into
     mats, translation i/j/k read as signed for >= nfft/2), the ligand placed
-    as in megadock_b200.synth.decoy_ca."""
+    as in megadock_b200.synth.decoy_ca: x_i = M y_i + b with y_i = ca_i -
+    lig_center, b = rec_center - t * gw.  The sum over atoms of
+    |M y_i + b - n_i|^2 is formed from 3x3 moments of y and the native n, so
+    the cost per pose does not grow with the chain length."""
     t = np.stack([poses["i"], poses["j"], poses["k"]], -1).astype(np.int64)
     t = np.where(t >= nfft // 2, t - nfft, t)
-    m = np.asarray(mats, np.float64)[poses["rot"]].reshape(-1, 3, 3)
-    x = np.asarray(lig_file_ca, np.float64) - lig_center
-    placed = np.einsum("pij,aj->pai", m, x) - t[:, None, :] * grid_width + rec_center
-    return np.sqrt(((placed - native_ca[None]) ** 2).sum(-1).mean(-1))
+    M = np.asarray(mats, np.float64)[poses["rot"]].reshape(-1, 3, 3)
+    b = np.asarray(rec_center, np.float64) - t * grid_width
+    y = np.asarray(lig_file_ca, np.float64) - lig_center
+    x = np.asarray(native_ca, np.float64)
+    n = len(y)
+    Syy = y.T @ y                      # sum y y^T
+    Syx = y.T @ x                      # sum y x^T
+    sy, sx, sxx = y.sum(0), x.sum(0), float((x * x).sum())
+    my = M @ sy                        # M sum y, per pose
+    ssq = (np.einsum("pij,jk,pik->p", M, Syy, M) + n * (b * b).sum(-1) + sxx + 2 * (b * my).sum(-1)
+           - 2 * np.einsum("pij,ji->p", M, Syx) - 2 * b @ sx)
+    return np.sqrt(np.maximum(ssq, 0.0) / n)
 
 
 class FitPair:

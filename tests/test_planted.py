@@ -41,3 +41,25 @@ def test_receptor_field_groups_sum_to_grid(built, pairs):
     # a single group holding every atom reproduces the grid bit for bit
     one = job.receptor_elec_groups(np.zeros(job.na_rec, np.int32), 1)
     assert np.array_equal(one[0], ri)
+
+
+def test_pose_rmsd_closed_form_matches_direct():
+    from megadock_b200 import POSE_DTYPE
+    from megadock_b200.fit import pose_rmsd
+    rng = np.random.default_rng(5)
+    q, _ = np.linalg.qr(rng.standard_normal((40, 3, 3)))
+    mats = q.reshape(40, 9).astype(np.float32)
+    ca = rng.standard_normal((57, 3)) * 10 + 3
+    lc, rc = np.array([1.0, -2.0, 0.5]), np.array([4.0, 4.0, -1.0])
+    nat = rng.standard_normal((57, 3)) * 10
+    poses = np.zeros(200, POSE_DTYPE)
+    poses["rot"] = rng.integers(0, 40, 200)
+    for f in ("i", "j", "k"):
+        poses[f] = rng.integers(0, 96, 200)
+    got = pose_rmsd(poses, mats, ca, lc, rc, nat, 96, 1.2)
+    t = np.stack([poses["i"], poses["j"], poses["k"]], -1)
+    t = np.where(t >= 48, t - 96, t)
+    M = mats.astype(np.float64)[poses["rot"]].reshape(-1, 3, 3)
+    placed = np.einsum("pij,aj->pai", M, ca - lc) - t[:, None, :] * 1.2 + rc
+    want = np.sqrt(((placed - nat) ** 2).sum(-1).mean(-1))
+    assert np.allclose(got, want, rtol=1e-9, atol=1e-9)
