@@ -492,12 +492,14 @@ def main():
     dom_ms_launch = stage_ms[dom] / nb_launches
     peak, peak_kind = _peaks()
     achieved = dom_bytes_launch / (dom_ms_launch * 1e-3) / 1e9
-    traffic = None
-    tfile = ROOT / "profiles" / "traffic_per_rotation.json"
-    if tfile.exists():
-        tr = json.loads(tfile.read_text()).get(names[dom])
-        if tr:
-            traffic = tr * batch
+    # DRAM bytes per rotation per stage from one ncu capture of this pipeline
+    # at N=128, 64 rotations per launch (dram__bytes_read.sum +
+    # dram__bytes_write.sum per launch / 64, profiles/ncu_dock_kernels_n128_b64.md);
+    # scaled by rotations per launch (R^, read once per launch by xline, adds
+    # 16.8 MB per launch and is left in the xline figure)
+    traffic_per_rotation = {"voxelize": 79.5e3, "plane_fwd": 7.54e6, "xline": 17.19e6, "plane_inv": 8.46e6,
+                            "merge": 3.3e3}
+    traffic = traffic_per_rotation[names[dom]] * batch if N_FFT == 128 else None
     value = world * nrot / (ms_batched * 1e-3)
     plain = world * nrot / (ms_plain * 1e-3)
     e2e = world * nrot / (ms_e2e * 1e-3)

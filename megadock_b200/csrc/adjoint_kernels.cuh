@@ -15,15 +15,18 @@
 namespace mdb {
 
 // Voxel index of the embedded grid at FFT position (a + d) mod N, or -1 when
-// it falls in the zero padding.
+// it falls in the zero padding.  a in [0, ng), d in [0, N), ng = N/2 and the
+// embedding offset N/4, so a + N/4 + d < 2N and one conditional subtraction
+// is the modulo.
 __device__ __forceinline__ int adj_cell(int a, int d, int N, int ng) {
-    const int off = N / 4;
-    int y = a + off + d;
-    y %= N;
-    if (y < 0) y += N;
-    y -= off;
-    return (y >= 0 && y < ng) ? y : -1;
+    int y = a + (N >> 2) + d;
+    if (y >= N) y -= N;
+    y -= N >> 2;
+    return ((unsigned)y < (unsigned)ng) ? y : -1;
 }
+
+// (N - d) mod N for d in [0, N): the shift that undoes d.
+__device__ __forceinline__ int adj_neg(int d, int N) { return d == 0 ? 0 : N - d; }
 
 // dRr/dRi += sum over the chunk's rotations of w_r * (Lr_r, Li_r)(x + t*_r).
 __global__ void k_adj_receptor(int N, int ng, int nb, const float *__restrict__ vr, const float *__restrict__ vi,
@@ -59,7 +62,8 @@ __global__ void k_adj_ligand(int N, int ng, int nsel, const int *__restrict__ se
     const int r = sel[m];
     const int i = (int)(c / ((size_t)ng * ng)), j = (int)((c / ng) % ng), k = (int)(c % ng);
     const int4 t = shift[r];
-    const int xi = adj_cell(i, -t.x, N, ng), xj = adj_cell(j, -t.y, N, ng), xk = adj_cell(k, -t.z, N, ng);
+    const int xi = adj_cell(i, adj_neg(t.x, N), N, ng), xj = adj_cell(j, adj_neg(t.y, N), N, ng),
+              xk = adj_cell(k, adj_neg(t.z, N), N, ng);
     float gr = 0.f, gi = 0.f;
     if (xi >= 0 && xj >= 0 && xk >= 0 && w[r] != 0.f) {
         const size_t x = ((size_t)xi * ng + xj) * ng + xk;
@@ -72,15 +76,19 @@ __global__ void k_adj_ligand(int N, int ng, int nsel, const int *__restrict__ se
 
 // dL/dq_a = sum_r w_r Ri(c_r(a) - t*_r), c_r(a) = the atom's charge cell in
 // rotation r (the same bit-exact rotation and cell rule as the voxelizer).
+// One warp per atom: lane l sums rotations l, l + 32, ... in order, then a
+// fixed shuffle tree adds the lanes, so the result does not depend on
+// scheduling.
 __global__ void k_adj_charge(LigandView L, GridView G, int N, int n_rot, const float *__restrict__ rotm,
                              const int4 *__restrict__ shift, const float *__restrict__ w,
                              const float *__restrict__ reci, float *__restrict__ dq) {
-    const int a = blockIdx.x * blockDim.x + threadIdx.x;
-    if (a >= L.na) return;
+    const int a = (int)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    if (a >= L.na) return;   // whole warps leave together
     const float4 at = __ldg(&L.atom[a]);
     const int ng = G.ng;
     float acc = 0.f;
-    for (int r = 0; r < n_rot; ++r) {
+    for (int r = lane; r < n_rot; r += 32) {
         const float wr = __ldg(&w[r]);
         if (wr == 0.f) continue;
         const float *m = rotm + 9 * (size_t)r;
@@ -91,11 +99,14 @@ __global__ void k_adj_charge(LigandView L, GridView G, int N, int n_rot, const f
         const int cj = charge_cell(rot_x(mm + 3, at.x, at.y, at.z), G.pad, G.gw, ng);
         const int ck = charge_cell(rot_x(mm + 6, at.x, at.y, at.z), G.pad, G.gw, ng);
         const int4 t = __ldg(&shift[r]);
-        const int xi = adj_cell(ci, -t.x, N, ng), xj = adj_cell(cj, -t.y, N, ng), xk = adj_cell(ck, -t.z, N, ng);
+        const int xi = adj_cell(ci, adj_neg(t.x, N), N, ng), xj = adj_cell(cj, adj_neg(t.y, N), N, ng),
+                  xk = adj_cell(ck, adj_neg(t.z, N), N, ng);
         if (xi < 0 || xj < 0 || xk < 0) continue;
         acc = fmaf(wr, __ldg(&reci[((size_t)xi * ng + xj) * ng + xk]), acc);
     }
-    dq[a] = acc;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if (lane == 0) dq[a] = acc;
 }
 
 // Score of one pose per block: sum_x Rr(x) Lr(x + t) + Ri(x) Li(x + t) over the

@@ -799,7 +799,7 @@ int adjoint_core(md_ctx *ctx, const float *rotmat, int n, const int4 *shift, con
     // charge gradient through the charge-cell assignment
     GridView G{ng, ctx->gw, (float)(ng * ctx->gw) / 2, ctx->d_gc, ctx->d_tw};
     LigandView L{ctx->na, ctx->d_atom, ctx->d_rad2, ctx->delta};
-    k_adj_charge<<<(ctx->na + 127) / 128, 128, 0, s>>>(L, G, N, n, d_rot, d_shift, d_w, ctx->d_recv + ng3, d_dq);
+    k_adj_charge<<<(ctx->na + 3) / 4, 128, 0, s>>>(L, G, N, n, d_rot, d_shift, d_w, ctx->d_recv + ng3, d_dq);
     if (n_lig > 0) {
         step(cudaMemcpyAsync(d_sel, lig_sel, sizeof(int) * n_lig, cudaMemcpyHostToDevice, s));
         k_adj_ligand<<<dim3(blocks, n_lig), thr, 0, s>>>(N, ng, n_lig, d_sel, ctx->d_recv, ctx->d_recv + ng3,
@@ -862,6 +862,11 @@ int md_adjoint_lse(md_ctx *ctx, const float *rotmat, int n_rot, const md_pose *t
     std::vector<float> w(n_rot);
     std::vector<int4> shift(n_rot);
     for (int r = 0; r < n_rot; ++r) {
+        if (top1[r].i < 0 || top1[r].i >= ctx->N || top1[r].j < 0 || top1[r].j >= ctx->N || top1[r].k < 0 ||
+            top1[r].k >= ctx->N) {
+            ctx->err = "pose translation outside [0, nf1)";
+            return MD_ERR_ARG;
+        }
         const bool live = top1[r].score > 0.f;
         w[r] = live ? (float)(std::exp(((double)top1[r].score - smax) / temperature) / z) : 0.f;
         shift[r] = make_int4(top1[r].i, top1[r].j, top1[r].k, 0);
