@@ -198,6 +198,22 @@ int md_job_grid_coord(const md_job *job, float *out);                 /* ng1 */
 int md_job_receptor_grids(const md_job *job, float *grid_r, float *grid_i); /* ng1^3 */
 int md_job_ligand_atoms(const md_job *job, float *xyz_centred, float *radius, float *charge);
 int md_job_receptor_atoms(const md_job *job, float *xyz, float *radius, float *charge, float *ace);
+/* Table mode (-tb), replacing the MPI job farm of src/mpidp.cpp:132-251,
+ * :300-551, :786-914 with a one-process queue on one GPU.  argv is the whole
+ * command line (-tb <table> [-ot n] [-rt n] [-wl n] [-lg log] [-pg prog] and
+ * the options passed to every job).  Jobs run in table order on ctx (NULL:
+ * a context on device 0), the next jobs' host preparation overlapping the
+ * GPU; the log (default ./master.log) gets the option echo, the JOB table
+ * and the Worker table in the reference's format.  Returns MD_OK when the
+ * queue ran (n_ok of n_jobs jobs ended with RET=0, and FILE=1 under -ot), or
+ * an error for a missing table, log or PARAM= line. */
+int md_table_mode(int argc, const char **argv);   /* 1 when argv has -tb */
+int md_table_run(int argc, const char **argv, md_ctx *ctx, int *n_ok, int *n_jobs);
+/* The argument vector of table job `job` (0-based) at attempt `retry`, one
+ * argument per line, then "#out <file>" (the -ot field, empty without -ot);
+ * job < 0 only counts the jobs into *n_jobs. */
+int md_table_expand(int argc, const char **argv, int job, int retry, char *buf, int buflen, int *n_jobs);
+
 /* Receptor::electro (src/receptor.cpp:258-346) split by atom group: grids
  * holds ngroups * ng1^3 floats; atom l adds its field to grid group[l]
  * (atoms with group[l] outside [0, ngroups) are left out).  Same search

@@ -1,12 +1,21 @@
 // megadock-b200: the MEGADOCK command line (src/main.cpp, src/control.cpp)
 // over the B200 pipeline.  Same flags (-R -L -o -N -t -F -v -D -r -e -d -a -b
-// -f ...), same .out file; one GPU (device 0), no CPU fallback.
+// -f ...), same .out file; one GPU (device 0), no CPU fallback.  With -tb it
+// is the table-mode driver (megadock-dp, src/mpidp.cpp) as one process.
 #include <chrono>
 #include <cstdio>
 
 #include "../../../include/md_b200.h"
 
 int main(int argc, char **argv) {
+    if (md_table_mode(argc, (const char **)argv)) {
+        // -tb: the table's jobs as a one-process queue (MEGADOCK's megadock-dp)
+        int ok = 0, n = 0;
+        const int rc = md_table_run(argc, (const char **)argv, nullptr, &ok, &n);
+        if (rc) return rc == MD_ERR_USAGE ? 255 : 1;
+        std::printf(" megadock-b200 table mode: %d of %d jobs ended normally\n", ok, n);
+        return ok == n ? 0 : 1;
+    }
     std::printf(" megadock-b200 (MEGADOCK 4.1.3 command line, B200 pipeline)\n\n");
     const auto t0 = std::chrono::steady_clock::now();
     md_job *job = nullptr;

@@ -6,6 +6,8 @@
 // drop-in contract.  Errors are returned, never exit()ed.
 #include <dlfcn.h>
 #include <getopt.h>
+
+#include <mutex>
 #include <unistd.h>
 
 #include <cstdio>
@@ -96,6 +98,10 @@ static std::string base_without_ext(std::string s) {
 }
 
 int parse_command_line(int argc, char **argv, Params &p, std::string &err, std::string &log) {
+    // getopt keeps its state in globals: one parse at a time (the table mode
+    // prepares jobs on several host threads)
+    static std::mutex getopt_lock;
+    std::lock_guard<std::mutex> hold(getopt_lock);
     p = Params();
     const std::string rb = "_r_b.pdb", lb = "_l_b.pdb", ru = "_r_u.pdb", lu = "_l_u.pdb";
     optind = 1;
