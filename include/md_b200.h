@@ -141,6 +141,16 @@ int md_adjoint_poses(md_ctx *ctx, const float *rotmat, int n, const md_pose *pos
  * score grid at that translation (FP32, fixed summation order). */
 int md_pose_scores(md_ctx *ctx, const float *rotmat, int n, const md_pose *poses, float *scores);
 
+/* Score terms for the detail output (Docking::output_detail,
+ * src/docking.cpp:456-898): for n poses (rotation rotmat[9p..], offsets
+ * tem3[3p..] = (3 ng1 - t) mod 2 ng1 of the translation t per axis), nine
+ * floats each in terms[9p..]: the direct sums of the rPSC, electrostatic and
+ * ACE products, then rPSC+, rPSC-, ELEC+, ELEC-, ACE+, ACE-.  rec_rpsc is the
+ * receptor's real grid without the ACE term (ng1^3, host); the real grid
+ * with it and the electrostatic grid are those given to md_receptor_fft.
+ * Sums in the reference's cell order, no FMA: the reference's floats. */
+int md_pose_terms(md_ctx *ctx, const float *rec_rpsc, const float *rotmat, int n, const int *tem3, float *terms);
+
 /* Ligand::rpscace + Ligand::electro (src/ligand.cpp:20-239) of one rotation,
  * computed by the device voxelizer; grid_r/grid_i receive ng1^3 floats. */
 int md_ligand_voxels(md_ctx *ctx, const float *rotmat9, float *grid_r, float *grid_i);

@@ -142,4 +142,59 @@ __global__ void k_pose_dot(int N, int ng, const float *__restrict__ recr, const 
     }
 }
 
+// Score terms of one pose per thread for the detail output
+// (src/docking.cpp:618-660, :733-812): the ligand cell l of the pose's
+// voxel grid meets receptor cell l + tem - ng on each axis, with
+// tem = (3 ng - t) mod 2 ng, over the same l, m, n ranges and in the same
+// order as the reference, every product rounded before it is added (no
+// FMA), so the float sums are the reference's.  terms[9 p ..]: direct sums of
+// rPSC, ELEC and ACE products, then rPSC+, rPSC-, ELEC+, ELEC-, ACE+, ACE-.
+__global__ void k_pose_terms(int ng, int n, const int4 *__restrict__ tem, const float *__restrict__ rec_r,
+                             const float *__restrict__ rec_rpsc, const float *__restrict__ rec_i,
+                             const float *__restrict__ vr, const float *__restrict__ vi, float *__restrict__ terms) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n) return;
+    const size_t ng2 = (size_t)ng * ng, ng3 = ng2 * ng;
+    const int4 tc = tem[p];
+    const int la = tc.x < ng ? ng - tc.x : 0, lb = tc.x < ng ? ng : 2 * ng - tc.x;
+    const int ma = tc.y < ng ? ng - tc.y : 0, mb = tc.y < ng ? ng : 2 * ng - tc.y;
+    const int na = tc.z < ng ? ng - tc.z : 0, nb = tc.z < ng ? ng : 2 * ng - tc.z;
+    const float *lr = vr + (size_t)p * ng3, *li = vi + (size_t)p * ng3;
+    float s_rpsc = 0.f, s_elec = 0.f, s_ace = 0.f;
+    float rp = 0.f, rm = 0.f, ep = 0.f, em = 0.f, ap = 0.f, am = 0.f;
+    for (int l = la; l < lb; ++l) {
+        const size_t rxc = ng2 * (size_t)(l + tc.x - ng), lxc = ng2 * (size_t)l;
+        for (int m = ma; m < mb; ++m) {
+            const size_t ryc = rxc + (size_t)ng * (m + tc.y - ng), lyc = lxc + (size_t)ng * m;
+            for (int k = na; k < nb; ++k) {
+                const size_t rzc = ryc + (size_t)(tc.z + k - ng), lzc = lyc + k;
+                const float a = __ldg(&rec_rpsc[rzc]), b = __ldg(&rec_r[rzc]), c = __ldg(&rec_i[rzc]);
+                const float x = __ldg(&lr[lzc]), y = __ldg(&li[lzc]);
+                const float rpsc = __fmul_rn(a, x);
+                const float elec = __fmul_rn(c, y);
+                const float ace = __fmul_rn(__fsub_rn(b, a), x);
+                s_rpsc = __fadd_rn(s_rpsc, rpsc);
+                s_elec = __fadd_rn(s_elec, elec);
+                s_ace = __fadd_rn(s_ace, ace);
+                if (rpsc < 0.f) rm = __fadd_rn(rm, rpsc);
+                else if (rpsc > 0.f) rp = __fadd_rn(rp, rpsc);
+                if (elec < 0.f) em = __fadd_rn(em, elec);
+                else if (elec > 0.f) ep = __fadd_rn(ep, elec);
+                if (ace < 0.f) am = __fadd_rn(am, ace);
+                else if (ace > 0.f) ap = __fadd_rn(ap, ace);
+            }
+        }
+    }
+    float *o = terms + 9 * (size_t)p;
+    o[0] = s_rpsc;
+    o[1] = s_elec;
+    o[2] = s_ace;
+    o[3] = rp;
+    o[4] = rm;
+    o[5] = ep;
+    o[6] = em;
+    o[7] = ap;
+    o[8] = am;
+}
+
 }  // namespace mdb

@@ -8,6 +8,8 @@
 //                  the score merge and the .out file (src/control.cpp:468-529,
 //                  src/docking.cpp:194-346, 399-453)
 #include <algorithm>
+#include <array>
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -75,6 +77,156 @@ const char *md_job_log(const md_job *job) { return job ? job->log.c_str() : ""; 
 
 void md_job_destroy(md_job *job) { delete job; }
 
+}  // extern "C"
+
+namespace {
+
+// Docking::output_detail (src/docking.cpp:456-898): the .detail and .csv
+// files.  Score terms come from md_pose_terms (the reference's summation
+// order on the GPU); RMSD, near-native flags and formatting follow the
+// reference on the host, including its use of the unrotated ligand
+// coordinates in the RMSD (only the translation enters it).
+int write_detail(md_job *job, md_ctx *ctx) {
+    const Params &p = job->p;
+    const int ng1 = job->ng1, nf1 = job->nf1;
+    const float gw = p.grid_width;
+    // receptor grid without the ACE term (the reference sets the ACE ratio to 0)
+    Params p0 = p;
+    p0.ace_ratio = 0.0f;
+    std::vector<float> rpsc, unused;
+    receptor_grids(job->rec, p0, job->gc, ng1, rpsc, unused);
+    float diff[3];
+    int cor[3];
+    for (int i = 0; i < 3; ++i) {
+        diff[i] = job->rec.center[i] - job->lig.center[i];
+        cor[i] = (int)std::round(diff[i] / gw);
+        if (cor[i] < 0) cor[i] += nf1;
+    }
+    // poses: 7 around the position that restores the input placement, then the top list
+    std::vector<int> tem;
+    std::vector<float> rot;
+    std::vector<std::array<int, 3>> cors;
+    float ident[9];
+    const float zero[3] = {0.f, 0.f, 0.f};
+    rotation_matrix(zero, ident);
+    int c[3] = {cor[0], cor[1], cor[2]};
+    for (int rank = 0; rank < 7; ++rank) {
+        if (rank == 1) c[0]--;
+        if (rank == 2) c[0] += 2;
+        if (rank == 3) { c[0]--; c[1]--; }
+        if (rank == 4) c[1] += 2;
+        if (rank == 5) { c[1]--; c[2]--; }
+        if (rank == 6) c[2] += 2;
+        cors.push_back({c[0], c[1], c[2]});
+        for (int k = 0; k < 3; ++k) tem.push_back((3 * ng1 - c[k]) % (2 * ng1));
+        rot.insert(rot.end(), ident, ident + 9);
+    }
+    for (const md_pose &q : job->top) {
+        const int t[3] = {q.i, q.j, q.k};
+        cors.push_back({q.i, q.j, q.k});
+        for (int k = 0; k < 3; ++k) tem.push_back((3 * ng1 - t[k]) % (2 * ng1));
+        float m[9];
+        rotation_matrix(&p.angles[3 * (size_t)q.rot], m);
+        rot.insert(rot.end(), m, m + 9);
+    }
+    const int n = (int)cors.size();
+    std::vector<float> terms((size_t)n * 9);
+    int rc = md_pose_terms(ctx, rpsc.data(), rot.data(), n, tem.data(), terms.data());
+    if (rc) {
+        job->err = md_last_error(ctx);
+        return rc;
+    }
+    // atom classes: 1 C-alpha, 2 backbone C or N, 0 others (src/protein.cpp:51-60)
+    const int na = job->lig.na();
+    std::vector<int> type(na);
+    int n_ca = 0, n_bb = 0;
+    for (int i = 0; i < na; ++i) {
+        const std::string &a = job->lig.atom_type[i];
+        type[i] = a.compare(0, 3, "CA ") == 0 ? 1 : (a.compare(0, 2, "C ") == 0 || a.compare(0, 2, "N ") == 0) ? 2 : 0;
+        n_ca += type[i] == 1;
+        n_bb += type[i] > 0;
+    }
+    auto rmsd_ca = [&](const int *tm) {
+        float lca = 0.0f, lbb = 0.0f;
+        for (int i = 0; i < na; ++i)
+            for (int k = 0; k < 3; ++k) {
+                if (type[i] <= 0) continue;
+                const float orig = job->lig.xyz[3 * (size_t)i + k];
+                const float moved = orig + gw * (tm[k] - ng1) + diff[k];
+                const double d2 = std::pow(moved - orig, 2.0);
+                if (type[i] == 1) lca = (float)(lca + d2);
+                lbb = (float)(lbb + d2);
+            }
+        (void)lbb;
+        return (float)std::sqrt(lca / n_ca);
+    };
+    FILE *fd = std::fopen(p.out_detail.c_str(), "w");
+    if (!fd) {
+        job->err = "[ERROR] Output_detail file [" + p.out_detail + "] not open!!";
+        return MD_ERR_IO;
+    }
+    FILE *fc = std::fopen(p.out_csv.c_str(), "w");
+    if (!fc) {
+        std::fclose(fd);
+        job->err = "[ERROR] Output_csv file [" + p.out_csv + "] not open!!";
+        return MD_ERR_IO;
+    }
+    std::fprintf(fd, "%d\t%.2f\n", nf1, gw);
+    std::fprintf(fd, "\t%f\t%f\t%f\n", 0.0f, 0.0f, 0.0f);
+    std::fprintf(fd, "%s\t%f\t%f\t%f\n", p.rec_file.c_str(), job->rec.center[0], job->rec.center[1],
+                 job->rec.center[2]);
+    std::fprintf(fd, "%s\t%f\t%f\t%f\n", p.lig_file.c_str(), job->lig.center[0], job->lig.center[1],
+                 job->lig.center[2]);
+    std::fprintf(fd, "\nElec score ratio: %6.2f\nACE  score ratio: %6.2f\n", p.elec_ratio, p.ace_ratio);
+    std::fprintf(fd, "\ncorrect position: angle = (%5.2f,%5.2f,%5.2f), trans = (%3d,%3d,%3d) \n\n", 0.0f, 0.0f,
+                 0.0f, cor[0], cor[1], cor[2]);
+    std::fprintf(fd, " *** score around correct position *** \n\n");
+    const char *cols = "Rank   Angle               Trans         total       rPSC     rPSC(+)  rPSC(-)  ELEC       "
+                       "RecACE     LCARMSD NearNat";
+    std::fprintf(fd, "%s\n", cols);
+    const float nn_thr = 5.0f;
+    for (int r = 0; r < 7; ++r) {
+        const float *t = &terms[9 * (size_t)r];
+        const float total = t[0] + t[1] + t[2];
+        const float rm = rmsd_ca(&tem[3 * (size_t)r]);
+        std::fprintf(fd, "%5d: (%5.2f,%5.2f,%5.2f) (%3d,%3d,%3d) %11.2f %8.0f %8.0f %8.0f %10.2f %10.2f %7.3f %7d\n",
+                     r + 1, 0.0f, 0.0f, 0.0f, cors[r][0], cors[r][1], cors[r][2], total, t[0], t[3], t[4], t[1],
+                     t[2], rm, rm < nn_thr ? 1 : 0);
+    }
+    std::fprintf(fd, "\n *** docking results *** \n\n%s\n", cols);
+    std::fprintf(fc, "Rank,Anglex,Angley,Anglez,Transi,Transj,Transk,total,rPSC,rPSC_gain,rPSC_penalty,ELEC ,RecACE,"
+                     "LCARMSD,NearNat\n");
+    const float pi = (float)(4.0 * std::atan(1.0));
+    for (size_t r = 0; r < job->top.size(); ++r) {
+        const size_t q = 7 + r;
+        const float *t = &terms[9 * q];
+        const float s_rpsc = t[3] + t[4], s_elec = t[5] + t[6], s_ace = t[7] + t[8];
+        const float total = s_rpsc + s_elec + s_ace;
+        float th[3];
+        for (int k = 0; k < 3; ++k) {
+            th[k] = p.angles[3 * (size_t)job->top[r].rot + k];
+            if (th[k] >= pi) th[k] = (float)(th[k] - pi * 2.0);
+        }
+        const float rm = rmsd_ca(&tem[3 * q]);
+        std::fprintf(fd, "%5d: (%5.2f,%5.2f,%5.2f) (%3d,%3d,%3d) %11.2f %8.0f %8.0f %8.0f %10.2f %10.2f %7.3f %7d\n",
+                     (int)r + 1, th[0], th[1], th[2], cors[q][0], cors[q][1], cors[q][2], total, s_rpsc, t[3], t[4],
+                     s_elec, s_ace, rm, rm < nn_thr ? 1 : 0);
+        std::fprintf(fc, "%d, %f,%f,%f,%d,%d,%d,%f,%f,%f,%f,%f,%f,%f,%d\n", (int)r + 1, th[0], th[1], th[2],
+                     cors[q][0], cors[q][1], cors[q][2], total, s_rpsc, t[3], t[4], s_elec, s_ace, rm,
+                     rm < nn_thr ? 1 : 0);
+    }
+    const bool ok = std::fclose(fd) == 0;
+    if (std::fclose(fc) != 0 || !ok) {
+        job->err = "[ERROR] writing the detail output";
+        return MD_ERR_IO;
+    }
+    return MD_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
 int md_job_run(md_job *job, md_ctx *ctx) {
     if (!job) return MD_ERR_ARG;
     md_ctx *own = nullptr;
@@ -106,6 +258,10 @@ int md_job_run(md_job *job, md_ctx *ctx) {
     job->top = job->poses;
     md_sort_poses(job->top.data(), (int)job->top.size(), job->p.num_output);
     job->top.resize(std::min((size_t)job->p.num_output, job->top.size()));
+    if (job->p.detail_output && (rc = write_detail(job, ctx))) {
+        if (own) md_ctx_destroy(own);
+        return rc;
+    }
     std::vector<PoseRec> recs;
     for (const md_pose &q : job->top) recs.push_back(PoseRec{q.score, q.rot, q.i, q.j, q.k});
     if ((rc = write_out_file(job->p.out_file, job->nf1, job->p.grid_width, job->rec, job->lig, job->p, recs,

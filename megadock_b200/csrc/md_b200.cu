@@ -976,6 +976,67 @@ int md_pose_scores(md_ctx *ctx, const float *rotmat, int n, const md_pose *poses
     return MD_OK;
 }
 
+int md_pose_terms(md_ctx *ctx, const float *rec_rpsc, const float *rotmat, int n, const int *tem3, float *terms) {
+    if (!ctx || !rec_rpsc || !rotmat || !tem3 || !terms || n < 1) return MD_ERR_ARG;
+    int rc = check_ready(ctx);
+    if (rc) return rc;
+    const int ng = ctx->ng;
+    for (int p = 0; p < 3 * n; ++p)
+        if (tem3[p] < 0 || tem3[p] >= 2 * ng) {
+            ctx->err = "pose offset outside [0, nf1)";
+            return MD_ERR_ARG;
+        }
+    MD_CUDA(cudaSetDevice(ctx->device));
+    const size_t ng3 = (size_t)ng * ng * ng;
+    // poses per launch: their voxel grids within about 1 GB
+    const int P = (int)std::max<size_t>(1, std::min<size_t>((size_t)n, ((size_t)1 << 30) / (8 * ng3)));
+    const int B = std::max(1, std::min(ctx->batch, P));
+    if ((rc = ensure_work(ctx, B, 1))) return rc;
+    float *d_rot = nullptr, *d_vox = nullptr, *d_terms = nullptr, *d_rpsc = nullptr;
+    int4 *d_tem = nullptr;
+    cudaError_t e = cudaSuccess;
+    auto step = [&](cudaError_t x) {
+        if (e == cudaSuccess) e = x;
+    };
+    std::vector<int4> tem(n);
+    for (int p = 0; p < n; ++p) tem[p] = make_int4(tem3[3 * p], tem3[3 * p + 1], tem3[3 * p + 2], 0);
+    step(cudaMalloc(&d_rot, sizeof(float) * 9 * n));
+    step(cudaMalloc(&d_tem, sizeof(int4) * n));
+    step(cudaMalloc(&d_terms, sizeof(float) * 9 * n));
+    step(cudaMalloc(&d_rpsc, sizeof(float) * ng3));
+    step(cudaMalloc(&d_vox, sizeof(float) * 2 * ng3 * P));
+    cudaStream_t s = ctx->stream;
+    step(cudaMemcpyAsync(d_rot, rotmat, sizeof(float) * 9 * n, cudaMemcpyHostToDevice, s));
+    step(cudaMemcpyAsync(d_tem, tem.data(), sizeof(int4) * n, cudaMemcpyHostToDevice, s));
+    step(cudaMemcpyAsync(d_rpsc, rec_rpsc, sizeof(float) * ng3, cudaMemcpyHostToDevice, s));
+    if (e == cudaSuccess) {
+        for (int p0 = 0; p0 < n; p0 += P) {
+            const int np = std::min(P, n - p0);
+            for (int b0 = 0; b0 < np; b0 += B) {
+                const int nb = std::min(B, np - b0);
+                // the chunk's grids at [b0, b0 + nb) of the P-pose buffers
+                launch_voxel_chunk(ctx, d_rot + 9 * (size_t)(p0 + b0), nb, d_vox + ng3 * b0,
+                                   d_vox + ng3 * ((size_t)P + b0));
+            }
+            k_pose_terms<<<(np + 31) / 32, 32, 0, s>>>(ng, np, d_tem + p0, ctx->d_recv, d_rpsc, ctx->d_recv + ng3,
+                                                      d_vox, d_vox + ng3 * P, d_terms + 9 * (size_t)p0);
+        }
+        step(cudaGetLastError());
+        step(cudaMemcpyAsync(terms, d_terms, sizeof(float) * 9 * n, cudaMemcpyDeviceToHost, s));
+        step(cudaStreamSynchronize(s));
+    }
+    cudaFree(d_rot);
+    cudaFree(d_tem);
+    cudaFree(d_terms);
+    cudaFree(d_rpsc);
+    cudaFree(d_vox);
+    if (e != cudaSuccess) {
+        ctx->err = std::string("pose terms: ") + cudaGetErrorString(e);
+        return MD_ERR_CUDA;
+    }
+    return MD_OK;
+}
+
 int md_ligand_voxels(md_ctx *ctx, const float *rotmat9, float *grid_r, float *grid_i) {
     if (!ctx || !rotmat9 || !grid_r || !grid_i) return MD_ERR_ARG;
     if (!ctx->N || !ctx->have_ligand) {
