@@ -38,7 +38,7 @@ def test_detail_matches_reference(built, gpu, pairs, tmp_path, name, flags):
     b = (tmp_path / "ref.detail").read_text().splitlines()
     assert len(a) == len(b)
     cut = a.index(" *** docking results *** ")
-    assert a[2:cut] == b[2:cut] and a[0] == b[0]          # lines 3-4 name the output paths' PDBs
+    assert a[:cut] == b[:cut]
     ra, rb = _rows(a[cut + 3:]), _rows(b[cut + 3:])
     common = set(ra) & set(rb)
     assert len(common) >= 0.9 * len(rb)
