@@ -224,6 +224,14 @@ int md_table_run(int argc, const char **argv, md_ctx *ctx, int *n_ok, int *n_job
  * job < 0 only counts the jobs into *n_jobs. */
 int md_table_expand(int argc, const char **argv, int job, int retry, char *buf, int buflen, int *n_jobs);
 
+/* .out consumers.  md_decoy_pdb writes the ligand PDB placed by pose number
+ * `decoy` (1-based) of out_file (the decoygen tool, src/decoygen.cpp:39-149);
+ * md_ligand_centres writes the placed ligand centre of every pose as
+ * "x, y, z" lines or pseudo-atom HETATM records (pdb_format = 1) to dest
+ * (NULL: standard output; the calcrg tool, src/calcrg.cpp:31-110). */
+int md_decoy_pdb(const char *out_file, const char *ligand_pdb, int decoy, const char *dest_pdb);
+int md_ligand_centres(const char *out_file, int pdb_format, const char *dest);
+
 /* Receptor::electro (src/receptor.cpp:258-346) split by atom group: grids
  * holds ngroups * ng1^3 floats; atom l adds its field to grid group[l]
  * (atoms with group[l] outside [0, ngroups) are left out).  Same search

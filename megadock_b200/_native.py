@@ -76,6 +76,8 @@ _PROTOS = {
     "md_job_ligand_atoms": (C.c_int, [_VP, _FP, _FP, _FP]),
     "md_job_receptor_atoms": (C.c_int, [_VP, _FP, _FP, _FP, _FP]),
     "md_job_receptor_elec_groups": (C.c_int, [_VP, _IP, C.c_int, _FP]),
+    "md_decoy_pdb": (C.c_int, [C.c_char_p, C.c_char_p, C.c_int, C.c_char_p]),
+    "md_ligand_centres": (C.c_int, [C.c_char_p, C.c_int, C.c_char_p]),
     "md_table_mode": (C.c_int, [C.c_int, C.POINTER(C.c_char_p)]),
     "md_table_run": (C.c_int, [C.c_int, C.POINTER(C.c_char_p), _VP, _IP, _IP]),
     "md_table_expand": (C.c_int, [C.c_int, C.POINTER(C.c_char_p), C.c_int, C.c_int, C.c_char_p, C.c_int, _IP]),
