@@ -108,6 +108,18 @@ int md_dock_pairs(md_ctx *runner, md_ctx *const *pairs, int npairs, const float 
 int md_dock_profile(md_ctx *ctx, const float *d_rotmat, int first_rot, int n_rot, int t, md_pose *d_out,
                     float *stage_ms, int *launches);
 
+/* Receptor::rpscace + Receptor::electro (src/receptor.cpp:20-346) on the
+ * device: the rPSC/ACE real grid and the electrostatic grid of na receptor
+ * atoms (coordinates centred on the receptor, radius, charge and ACE value
+ * per atom; -a, -d and -e values), bit-exact with the reference's CPU code
+ * for grids up to ng1 = 96.  make_receptor = 1 also makes them this
+ * context's receptor (R^ for md_dock, and the grids for the adjoint), as
+ * md_receptor_fft would; grid_r / grid_i (ng1^3 host floats, may be NULL)
+ * receive a copy.  Needs md_set_grid. */
+int md_receptor_build(md_ctx *ctx, int na, const float *xyz_centred, const float *radius, const float *charge,
+                      const float *ace, float rec_core, float ace_ratio, float elec_ratio, int make_receptor,
+                      float *grid_r, float *grid_i);
+
 /* Adjoint (no counterpart in the reference, whose scores are not
  * differentiated): gradient of the smooth loss
  *     L = T * log(sum_r exp(s_r / T))

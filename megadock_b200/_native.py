@@ -56,6 +56,8 @@ _PROTOS = {
     "md_adjoint_poses": (C.c_int, [_VP, _FP, C.c_int, _VP, _FP, _FP, _FP, _FP, _IP, C.c_int, _FP, _FP]),
     "md_pose_scores": (C.c_int, [_VP, _FP, C.c_int, _VP, _FP]),
     "md_pose_terms": (C.c_int, [_VP, _FP, _FP, C.c_int, _IP, _FP]),
+    "md_receptor_build": (C.c_int, [_VP, C.c_int, _FP, _FP, _FP, _FP, C.c_float, C.c_float, C.c_float, C.c_int,
+                                    _FP, _FP]),
     "md_adjoint_lse": (C.c_int, [_VP, _FP, C.c_int, _VP, C.c_float, C.c_float, C.POINTER(C.c_double), _FP, _FP, _FP,
                                  C.POINTER(C.c_double), _IP, C.c_int, _FP, _FP]),
     "md_dock_profile": (C.c_int, [_VP, _VP, C.c_int, C.c_int, C.c_int, _VP, _FP, _IP]),

@@ -66,9 +66,15 @@ int md_job_create(int argc, const char **argv, md_job **out) {
     job->ng1 = std::max(job->rec.num_grid, job->lig.num_grid);
     job->nf1 = job->ng1 * 2;
     job->gc = grid_coordinates(job->ng1, job->p.grid_width);
-    receptor_grids(job->rec, job->p, job->gc, job->ng1, job->rec_r, job->rec_i);
     job->lig_xyz = centred_coordinates(job->lig);
     return MD_OK;
+}
+
+// Host receptor grids, built on first use by the accessors that return them
+// (the docking path builds them on the device).
+static void host_receptor(const md_job *job) {
+    md_job *j = const_cast<md_job *>(job);
+    if (j->rec_r.empty()) receptor_grids(j->rec, j->p, j->gc, j->ng1, j->rec_r, j->rec_i);
 }
 
 const char *md_job_error(const md_job *job) { return job ? job->err.c_str() : "null job"; }
@@ -91,10 +97,16 @@ int write_detail(md_job *job, md_ctx *ctx) {
     const int ng1 = job->ng1, nf1 = job->nf1;
     const float gw = p.grid_width;
     // receptor grid without the ACE term (the reference sets the ACE ratio to 0)
-    Params p0 = p;
-    p0.ace_ratio = 0.0f;
-    std::vector<float> rpsc, unused;
-    receptor_grids(job->rec, p0, job->gc, ng1, rpsc, unused);
+    std::vector<float> rpsc((size_t)ng1 * ng1 * ng1);
+    {
+        const std::vector<float> xyz = centred_coordinates(job->rec);
+        int rc = md_receptor_build(ctx, job->rec.na(), xyz.data(), job->rec.radius.data(), job->rec.charge.data(),
+                                   job->rec.ace.data(), p.rec_core, 0.0f, p.elec_ratio, 0, rpsc.data(), nullptr);
+        if (rc) {
+            job->err = md_last_error(ctx);
+            return rc;
+        }
+    }
     float diff[3];
     int cor[3];
     for (int i = 0; i < 3; ++i) {
@@ -245,7 +257,14 @@ int md_job_run(md_job *job, md_ctx *ctx) {
     };
     int rc;
     if ((rc = md_set_grid(ctx, job->nf1, job->p.grid_width, job->gc.data()))) return fail(rc);
-    if ((rc = md_receptor_fft(ctx, job->rec_r.data(), job->rec_i.data()))) return fail(rc);
+    {
+        // receptor grids and R^ on the device
+        const std::vector<float> xyz = centred_coordinates(job->rec);
+        if ((rc = md_receptor_build(ctx, job->rec.na(), xyz.data(), job->rec.radius.data(), job->rec.charge.data(),
+                                    job->rec.ace.data(), job->p.rec_core, job->p.ace_ratio, job->p.elec_ratio, 1,
+                                    nullptr, nullptr)))
+            return fail(rc);
+    }
     if ((rc = md_ligand_data(ctx, job->lig.na(), job->lig_xyz.data(), job->lig.radius.data(),
                              job->lig.charge.data(), job->p.lig_core)))
         return fail(rc);
@@ -297,6 +316,7 @@ int md_job_grid_coord(const md_job *job, float *out) {
 
 int md_job_receptor_grids(const md_job *job, float *r, float *i) {
     if (!job || !r || !i) return MD_ERR_ARG;
+    host_receptor(job);
     std::copy(job->rec_r.begin(), job->rec_r.end(), r);
     std::copy(job->rec_i.begin(), job->rec_i.end(), i);
     return MD_OK;
@@ -304,6 +324,7 @@ int md_job_receptor_grids(const md_job *job, float *r, float *i) {
 
 int md_job_receptor_elec_groups(const md_job *job, const int *group, int ngroups, float *grids) {
     if (!job || !group || ngroups < 1 || !grids) return MD_ERR_ARG;
+    host_receptor(job);
     receptor_electro(job->rec, job->p, job->gc, job->ng1, job->rec_r, group, ngroups, grids);
     return MD_OK;
 }

@@ -23,6 +23,7 @@
 
 #include "../../include/md_b200.h"
 #include "adjoint_kernels.cuh"
+#include "receptor_kernels.cuh"
 #include "dock_kernels.cuh"
 
 using namespace mdb;
@@ -526,6 +527,136 @@ int md_receptor_fft(md_ctx *ctx, const float *grid_r, const float *grid_i) {
         return MD_ERR_CUDA;
     }
     ctx->have_receptor = true;
+    return MD_OK;
+}
+
+int md_receptor_build(md_ctx *ctx, int na, const float *xyz_centred, const float *radius, const float *charge,
+                      const float *ace, float rec_core, float ace_ratio, float elec_ratio, int make_receptor,
+                      float *grid_r, float *grid_i) {
+    if (!ctx || na < 1 || !xyz_centred || !radius || !charge || !ace) return MD_ERR_ARG;
+    if (!ctx->N) {
+        ctx->err = "md_set_grid has not been called";
+        return MD_ERR_STATE;
+    }
+    const int ng = ctx->ng;
+    if (ng > kRecMaxNg) {
+        ctx->err = "receptor grids on the device are built for ng1 <= 96";
+        return MD_ERR_SIZE;
+    }
+    MD_CUDA(cudaSetDevice(ctx->device));
+    if (make_receptor) {
+        int rc = ensure_work(ctx, std::max(1, ctx->batch), 1);
+        if (rc) return rc;
+    }
+    const size_t ng3 = (size_t)ng * ng * ng;
+    const float open_space = -7777.0f;
+    // host copies of the two grid-coordinate values the reference reads
+    std::vector<float> gc(ng);
+    MD_CUDA(cudaMemcpy(gc.data(), ctx->d_gc, sizeof(float) * ng, cudaMemcpyDeviceToHost));
+    RecParams P;
+    P.ng = ng;
+    P.na = na;
+    P.gw = ctx->gw;
+    P.width = gc[1] - gc[0];
+    P.eps_core = rec_core;
+    P.e_ratio = elec_ratio;
+    P.cpg = -1 * P.width * 80.0f / (-2800.0f * elec_ratio);
+    P.ace_ratio = (double)ace_ratio;
+    P.reach_core = (int)((2.4 + ctx->gw - 0.01) / ctx->gw);
+    P.reach_shell = (int)((12 + ctx->gw - 0.01) / ctx->gw);
+    float *d_xyz = nullptr, *d_rad = nullptr, *d_q = nullptr, *d_ace = nullptr, *d_grid = nullptr;
+    RecAtom *d_atoms = nullptr;
+    int *d_cnt = nullptr, *d_start = nullptr, *d_list = nullptr;
+    cudaError_t e = cudaSuccess;
+    auto step = [&](cudaError_t x) {
+        if (e == cudaSuccess) e = x;
+    };
+    auto cleanup = [&]() {
+        cudaFree(d_xyz);
+        cudaFree(d_rad);
+        cudaFree(d_q);
+        cudaFree(d_ace);
+        cudaFree(d_atoms);
+        cudaFree(d_cnt);
+        cudaFree(d_start);
+        cudaFree(d_list);
+        if (!make_receptor) cudaFree(d_grid);
+    };
+    cudaStream_t s = ctx->stream;
+    step(cudaMalloc(&d_xyz, sizeof(float) * 3 * na));
+    step(cudaMalloc(&d_rad, sizeof(float) * na));
+    step(cudaMalloc(&d_q, sizeof(float) * na));
+    step(cudaMalloc(&d_ace, sizeof(float) * na));
+    step(cudaMalloc(&d_atoms, sizeof(RecAtom) * na));
+    step(cudaMalloc(&d_cnt, sizeof(int) * (ng * ng + 1)));
+    step(cudaMalloc(&d_start, sizeof(int) * (ng * ng + 1)));
+    if (make_receptor) d_grid = ctx->d_recv;
+    else step(cudaMalloc(&d_grid, sizeof(float) * 2 * ng3));
+    if (e != cudaSuccess) {
+        cleanup();
+        ctx->err = std::string("receptor grids: ") + cudaGetErrorString(e);
+        return MD_ERR_CUDA;
+    }
+    float *d_r = d_grid, *d_i = d_grid + ng3;
+    step(cudaMemcpyAsync(d_xyz, xyz_centred, sizeof(float) * 3 * na, cudaMemcpyHostToDevice, s));
+    step(cudaMemcpyAsync(d_rad, radius, sizeof(float) * na, cudaMemcpyHostToDevice, s));
+    step(cudaMemcpyAsync(d_q, charge, sizeof(float) * na, cudaMemcpyHostToDevice, s));
+    step(cudaMemcpyAsync(d_ace, ace, sizeof(float) * na, cudaMemcpyHostToDevice, s));
+    step(cudaMemsetAsync(d_r, 0, sizeof(float) * ng3, s));
+    const int rows = ng * ng;
+    const size_t sweep_smem = sizeof(RowMask) * rows;
+    step(cudaFuncSetAttribute(k_rec_sweep, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)(sizeof(RowMask) * kRecMaxNg * kRecMaxNg)));
+    const int cells_blocks = (int)((ng3 + 255) / 256);
+    std::vector<int> cnt(rows + 1), start(rows + 1);
+    auto scan = [&](int n) {   // counts -> starts on the host (n + 1 entries)
+        step(cudaMemcpyAsync(cnt.data(), d_cnt, sizeof(int) * n, cudaMemcpyDeviceToHost, s));
+        step(cudaStreamSynchronize(s));
+        start[0] = 0;
+        for (int r = 0; r < n; ++r) start[r + 1] = start[r] + cnt[r];
+        step(cudaMemcpyAsync(d_start, start.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice, s));
+        return start[n];
+    };
+    if (e == cudaSuccess) {
+        k_rec_prep<<<(na + 255) / 256, 256, 0, s>>>(P, d_xyz, d_rad, d_q, d_ace, d_atoms);
+        k_rec_core<<<na, 128, 0, s>>>(P, d_atoms, ctx->d_gc, d_r);
+        k_rec_rays<<<(3 * rows + 255) / 256, 256, 0, s>>>(P, d_r, open_space);
+        for (int sweep = 0; sweep < 2; ++sweep) k_rec_sweep<<<1, 1024, sweep_smem, s>>>(P, d_r, open_space);
+        k_rec_final<<<cells_blocks, 256, 0, s>>>(P, d_r, open_space);
+        // surface shell over per-row atom lists
+        k_rec_rows<<<(rows + 127) / 128, 128, 0, s>>>(P, d_atoms, ctx->d_gc, d_cnt, nullptr, nullptr);
+        const int nlist = scan(rows);
+        step(cudaMalloc(&d_list, sizeof(int) * std::max(1, nlist)));
+        if (e == cudaSuccess) {
+            k_rec_rows<<<(rows + 127) / 128, 128, 0, s>>>(P, d_atoms, ctx->d_gc, d_cnt, d_start, d_list);
+            k_rec_shell<<<cells_blocks, 256, 0, s>>>(P, d_atoms, ctx->d_gc, d_start, d_list, d_r);
+            step(cudaGetLastError());
+            step(cudaStreamSynchronize(s));
+            cudaFree(d_list);
+            d_list = nullptr;
+        }
+        // electrostatics over per-plane charged-atom lists
+        if (e == cudaSuccess) {
+            k_rec_planes<<<(ng + 63) / 64, 64, 0, s>>>(P, d_atoms, d_cnt, nullptr, nullptr);
+            const int nplane = scan(ng);
+            step(cudaMalloc(&d_list, sizeof(int) * std::max(1, nplane)));
+        }
+        if (e == cudaSuccess) {
+            k_rec_planes<<<(ng + 63) / 64, 64, 0, s>>>(P, d_atoms, d_cnt, d_start, d_list);
+            k_rec_elec<<<cells_blocks, 256, 0, s>>>(P, d_atoms, ctx->d_gc, d_start, d_list, d_r, d_i);
+            if (make_receptor) launch_receptor(ctx, d_r, d_i);
+            step(cudaGetLastError());
+        }
+        if (grid_r) step(cudaMemcpyAsync(grid_r, d_r, sizeof(float) * ng3, cudaMemcpyDeviceToHost, s));
+        if (grid_i) step(cudaMemcpyAsync(grid_i, d_i, sizeof(float) * ng3, cudaMemcpyDeviceToHost, s));
+        step(cudaStreamSynchronize(s));
+    }
+    cleanup();
+    if (e != cudaSuccess) {
+        ctx->err = std::string("receptor grids: ") + cudaGetErrorString(e);
+        return MD_ERR_CUDA;
+    }
+    if (make_receptor) ctx->have_receptor = true;
     return MD_OK;
 }
 

@@ -49,6 +49,24 @@ class FFTProcess:
         i = np.ascontiguousarray(grid_i, dtype=np.float32)
         _check(N.lib().md_receptor_fft(self._h, N.fptr(r), N.fptr(i)), self._h)
 
+    def receptor_build(self, xyz_centred, radius, charge, ace, rec_core=-45.0, ace_ratio=1.0, elec_ratio=1.0,
+                       make_receptor=True, return_grids=False):
+        """Receptor grids built on the device (md_receptor_build); with
+        make_receptor they become this context's receptor, like receptor_fft."""
+        xyz = np.ascontiguousarray(xyz_centred, dtype=np.float32).reshape(-1)
+        rad = np.ascontiguousarray(radius, dtype=np.float32)
+        q = np.ascontiguousarray(charge, dtype=np.float32)
+        a = np.ascontiguousarray(ace, dtype=np.float32)
+        ng = self.num_fft // 2
+        gr = np.zeros(ng ** 3, np.float32) if return_grids else None
+        gi = np.zeros(ng ** 3, np.float32) if return_grids else None
+        _check(N.lib().md_receptor_build(self._h, len(rad), N.fptr(xyz), N.fptr(rad), N.fptr(q), N.fptr(a),
+                                         float(rec_core), float(ace_ratio), float(elec_ratio), int(make_receptor),
+                                         N.fptr(gr) if gr is not None else None,
+                                         N.fptr(gi) if gi is not None else None), self._h)
+        if return_grids:
+            return gr.reshape((ng,) * 3), gi.reshape((ng,) * 3)
+
     def receptor_spectrum(self) -> np.ndarray:
         n3 = self.num_fft ** 3
         re = np.zeros(n3, np.float32)
