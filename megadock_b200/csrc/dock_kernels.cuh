@@ -28,6 +28,10 @@
 namespace mdb {
 
 constexpr int kNT = 512;          // threads per CTA for the plane kernels
+#ifndef MDB_K1_NT
+#define MDB_K1_NT 1024
+#endif
+constexpr int kNT1 = MDB_K1_NT;   // threads per CTA of the forward plane kernel (one CTA per SM)
 constexpr int kLT = 32;           // lines per CTA in the x-line kernel
 constexpr int kMaxLigAtoms = 32768;
 
@@ -120,29 +124,94 @@ __device__ void vox_mark(VoxShared<NG> &vs, const MarkEntry *__restrict__ rec, i
         if (i < 0 || i >= ng || i < me.box.x - 2 || i > me.box.x + 2 || j < 0 || j >= ng) continue;
         const float rc2 = me.pos.w, rs2 = __int_as_float(me.box.w);
         const float d2 = __fadd_rn(sqdist(me.pos.x, __ldg(&G.gc[i])), sqdist(me.pos.y, __ldg(&G.gc[j])));
-        uint32_t cbits[W], sbits[W];
-#pragma unroll
-        for (int w = 0; w < W; ++w) cbits[w] = sbits[w] = 0u;
+        // d3 = d2 + dz^2 >= d2 and R^2 <= 1.5 R^2: a row outside the core
+        // disc has no cell in either sphere
+        if (!(d2 < rc2)) continue;
+        // the row's (at most 5) cells as bits of a 64-bit window from word wb
         const int ka = max(me.box.z - 2, 0), kb = min(me.box.z + 3, ng);
+        const int wb = ka >> 5;
+        unsigned long long cm = 0ull, sm = 0ull;
         for (int k = ka; k < kb; ++k) {
             const float d3 = __fadd_rn(d2, sqdist(me.pos.z, __ldg(&G.gc[k])));
-#pragma unroll
-            for (int w = 0; w < W; ++w) {
-                if ((k >> 5) == w) {
-                    if (d3 < rc2) cbits[w] |= 1u << (k & 31);
-                    if (d3 < rs2) sbits[w] |= 1u << (k & 31);
-                }
-            }
+            const unsigned long long bit = 1ull << (k - 32 * wb);
+            if (d3 < rc2) cm |= bit;
+            if (d3 < rs2) sm |= bit;
         }
         const int slot = i - p + 2;
         const bool do_surf = (i >= p - 1 && i <= p + 1);
-#pragma unroll
-        for (int w = 0; w < W; ++w) {
-            if (cbits[w]) atomicOr(&vs.core[slot][j * W + w], cbits[w]);
-            if (do_surf && sbits[w]) atomicOr(&vs.surf[slot - 1][j * W + w], sbits[w]);
+        uint32_t *crow = &vs.core[slot][j * W + wb];
+        if ((uint32_t)cm) atomicOr(crow, (uint32_t)cm);
+        if (cm >> 32) atomicOr(crow + 1, (uint32_t)(cm >> 32));
+        if (do_surf) {
+            uint32_t *srow = &vs.surf[slot - 1][j * W + wb];
+            if ((uint32_t)sm) atomicOr(srow, (uint32_t)sm);
+            if (sm >> 32) atomicOr(srow + 1, (uint32_t)(sm >> 32));
         }
     }
     __syncthreads();
+}
+
+// Word-parallel form of vox_code: the class bits of 32 cells (row q, word w)
+// of plane p at once.  c2 = "value delta", c1 = "value 1.0".
+template <int NG>
+__device__ __forceinline__ uint32_t vw_core(const VoxShared<NG> &vs, int slot, int q, int w) {
+    constexpr int W = VoxShared<NG>::W;
+    return (q < 0 || q >= NG || w < 0 || w >= W) ? 0u : vs.core[slot][q * W + w];
+}
+
+template <int NG>
+__device__ __forceinline__ uint32_t vw_surf(const VoxShared<NG> &vs, int slot, int q, int w) {
+    constexpr int W = VoxShared<NG>::W;
+    return (q < 0 || q >= NG || w < 0 || w >= W) ? 0u : vs.surf[slot - 1][q * W + w];
+}
+
+// bits s of word w with 1 <= s <= ng - 2
+__device__ __forceinline__ uint32_t vw_inner(int w, int ng) {
+    uint32_t m = 0xffffffffu;
+    const int s0 = 32 * w;
+    if (s0 < 1) m &= ~1u;
+    const int hi = ng - 2 - s0;   // last kept bit
+    if (hi < 0) return 0u;
+    if (hi < 31) m &= (2u << hi) - 1u;
+    return m;
+}
+
+// core cells of (slot, q, w) that survive the scrape (vox_surv)
+template <int NG>
+__device__ __forceinline__ uint32_t vw_surv(const VoxShared<NG> &vs, int slot, int i, int q, int w, int ng) {
+    const uint32_t c = vw_core<NG>(vs, slot, q, w);
+    if (!c) return 0u;
+    const uint32_t left = (c << 1) | (vw_core<NG>(vs, slot, q, w - 1) >> 31);    // core at s - 1
+    const uint32_t right = (c >> 1) | (vw_core<NG>(vs, slot, q, w + 1) << 31);   // core at s + 1
+    const uint32_t nb = vw_core<NG>(vs, slot - 1, q, w) & vw_core<NG>(vs, slot + 1, q, w) &
+                        vw_core<NG>(vs, slot, q - 1, w) & vw_core<NG>(vs, slot, q + 1, w) & left & right;
+    const bool inner_iq = i >= 1 && i <= ng - 2 && q >= 1 && q <= ng - 2;
+    const uint32_t interior = inner_iq ? vw_inner(w, ng) : 0u;
+    return c & (~interior | nb);
+}
+
+// cells of class 0 (neither a surviving core cell nor a surface cell)
+template <int NG>
+__device__ __forceinline__ uint32_t vw_empty(const VoxShared<NG> &vs, int slot, int i, int q, int w, int ng) {
+    return ~(vw_surv<NG>(vs, slot, i, q, w, ng) | vw_surf<NG>(vs, slot, q, w));
+}
+
+template <int NG>
+__device__ __forceinline__ void vox_code_words(const VoxShared<NG> &vs, int p, int q, int w, int ng,
+                                               bool general_delta, uint32_t &c2, uint32_t &c1) {
+    const uint32_t surv = vw_surv<NG>(vs, 2, p, q, w, ng);
+    c2 = surv;
+    c1 = vw_surf<NG>(vs, 2, q, w) & ~surv;
+    if (!general_delta || !surv) return;
+    if (!(p >= 1 && p <= ng - 2 && q >= 1 && q <= ng - 2)) return;
+    const uint32_t e0 = vw_empty<NG>(vs, 2, p, q, w, ng);
+    const uint32_t es = (e0 << 1) | (vw_empty<NG>(vs, 2, p, q, w - 1, ng) >> 31) | (e0 >> 1) |
+                        (vw_empty<NG>(vs, 2, p, q, w + 1, ng) << 31);
+    const uint32_t ez = vw_empty<NG>(vs, 1, p - 1, q, w, ng) | vw_empty<NG>(vs, 3, p + 1, q, w, ng) |
+                        vw_empty<NG>(vs, 2, p, q - 1, w, ng) | vw_empty<NG>(vs, 2, p, q + 1, w, ng);
+    const uint32_t demote = surv & vw_inner(w, ng) & (es | ez);
+    c2 = surv & ~demote;
+    c1 |= demote;
 }
 
 // Core bit survives the swollen-surface scrape (src/ligand.cpp:110-134):
@@ -307,10 +376,13 @@ __global__ void __launch_bounds__(kNT0)
     const int *ss = sstart + (size_t)b * (NBS + 1);
     const int lo = ss[max(p - reach + kReach, 0)], hi = ss[min(p + reach + kReach + 1, NBS)];
     vox_mark<NG>(vs, rec + (size_t)b * L.na, lo, hi, G, p, gd);
-    for (int c = tid; c < NG * NG; c += blockDim.x) {
-        const int q = c / NG, s2 = c % NG;
-        const int code = vox_code<NG>(vs, p, q, s2, NG, gd);
-        if (code) atomicOr(&ob[2 - code][q * W + (s2 >> 5)], 1u << (s2 & 31));
+    for (int c = tid; c < NG * W; c += blockDim.x) {
+        const int q = c / W, w = c % W;
+        uint32_t c2, c1;
+        vox_code_words<NG>(vs, p, q, w, NG, gd, c2, c1);
+        const uint32_t valid = (32 * w + 32 <= NG) ? 0xffffffffu : ((1u << (NG - 32 * w)) - 1u);
+        ob[0][q * W + w] = c2 & valid;
+        ob[1][q * W + w] = c1 & valid;
     }
     // charges of this plane, in atom order: the first entry of each cell sums
     // that cell's entries in order
@@ -341,7 +413,7 @@ __global__ void __launch_bounds__(kNT0)
 // MODE 2: like MODE 0 but store the voxel plane itself (ng x ng real and
 //         imaginary parts) for parity checks; no FFT.
 template <int N, int MODE>
-__global__ void __launch_bounds__(kNT, 1)
+__global__ void __launch_bounds__(kNT1, 1)
     k_plane_fwd(LigandView L, GridView G, const uint32_t *__restrict__ vbits, const int2 *__restrict__ qlist,
                 const int *__restrict__ qcount, const float *__restrict__ src_r, const float *__restrict__ src_i,
                 float2 *__restrict__ A, float *__restrict__ vox_r, float *__restrict__ vox_i) {
@@ -398,17 +470,17 @@ __global__ void __launch_bounds__(kNT, 1)
     }
     __syncthreads();
     {
-        constexpr int IPT = (NG * R1 + kNT - 1) / kNT;
+        constexpr int IPT = (NG * R1 + kNT1 - 1) / kNT1;
         float2 reg[IPT][R2];
 #pragma unroll
         for (int r = 0; r < IPT; ++r) {
-            const int it = tid + r * kNT;
+            const int it = tid + r * kNT1;
             if (it < NG * R1) fft_phase2<N, -1>(S + ((it % NG) + OFF) * PITCH, 1, it / NG, reg[r]);
         }
         __syncthreads();
 #pragma unroll
         for (int r = 0; r < IPT; ++r) {
-            const int it = tid + r * kNT;
+            const int it = tid + r * kNT1;
             if (it < NG * R1) {
                 float2 *row = S + ((it % NG) + OFF) * PITCH;
                 const int u = it / NG;

@@ -165,7 +165,7 @@ struct Sized {
     static void receptor(md_ctx *c, const float *d_r, const float *d_i) {
         GridView G{c->ng, c->gw, 0.f, c->d_gc, c->d_tw};
         LigandView L{0, nullptr, nullptr, 1.f};
-        k_plane_fwd<N, 1><<<dim3(NG, 1), kNT, smem_fwd(), c->stream>>>(L, G, nullptr, nullptr, nullptr, d_r, d_i,
+        k_plane_fwd<N, 1><<<dim3(NG, 1), kNT1, smem_fwd(), c->stream>>>(L, G, nullptr, nullptr, nullptr, d_r, d_i,
                                                                         c->ws[0].A, nullptr, nullptr);
         k_xline_rec<N><<<dim3(N * TILES, 1), kNT, 0, c->stream>>>(G, c->ws[0].A, c->d_Rh);
     }
@@ -185,7 +185,7 @@ struct Sized {
         LigandView L{c->na, c->d_atom, c->d_rad2, c->delta};
         const WorkSet &w = c->ws[0];
         voxelize(c, w, d_rot9, nb, c->stream);
-        k_plane_fwd<N, 2><<<dim3(NG, nb), kNT, smem_fwd(), c->stream>>>(L, G, w.vbits, w.qlist, w.qcount, nullptr,
+        k_plane_fwd<N, 2><<<dim3(NG, nb), kNT1, smem_fwd(), c->stream>>>(L, G, w.vbits, w.qlist, w.qcount, nullptr,
                                                                          nullptr, nullptr, d_vr, d_vi);
     }
 
@@ -194,7 +194,7 @@ struct Sized {
         LigandView L{c->na, c->d_atom, c->d_rad2, c->delta};
         const WorkSet &w = c->ws[0];
         voxelize(c, w, d_rot9, 1, c->stream);
-        k_plane_fwd<N, 2><<<dim3(NG, 1), kNT, smem_fwd(), c->stream>>>(L, G, w.vbits, w.qlist, w.qcount, nullptr,
+        k_plane_fwd<N, 2><<<dim3(NG, 1), kNT1, smem_fwd(), c->stream>>>(L, G, w.vbits, w.qlist, w.qcount, nullptr,
                                                                         nullptr, nullptr, d_vr, d_vi);
     }
 
@@ -222,7 +222,7 @@ struct Sized {
         const float nf3f = (float)((long long)N * N * N);
         voxelize(c, w, d_rot9, nb, s);
         if (ev) cudaEventRecord(ev[1], s);
-        k_plane_fwd<N, 0><<<dim3(NG, nb), kNT, smem_fwd(), s>>>(L, G, w.vbits, w.qlist, w.qcount, nullptr, nullptr,
+        k_plane_fwd<N, 0><<<dim3(NG, nb), kNT1, smem_fwd(), s>>>(L, G, w.vbits, w.qlist, w.qcount, nullptr, nullptr,
                                                                 w.A, nullptr, nullptr);
         if (ev) cudaEventRecord(ev[2], s);
         k_xline_herm<N><<<dim3(NH * TILES, nb), kNT, smem_xline(), s>>>(G, w.A, c->d_Rh, w.G);
