@@ -210,6 +210,12 @@ void md_job_destroy(md_job *job);
 /* Control::execute (src/control.cpp:468-529): dock every rotation on ctx and
  * write the .out file.  ctx may be NULL (a context on device 0 is made). */
 int md_job_run(md_job *job, md_ctx *ctx);
+/* The output half of md_job_run for poses docked elsewhere (for example
+ * gathered from several GPUs): the n = n_rot * t poses in rotation-major
+ * order are merged (FFTProcess::sort_index, src/fft_process.cpp:469-479) and
+ * written as the .out (Docking::output, src/docking.cpp:399-453); with -O and
+ * a context the .detail/.csv files too. */
+int md_job_write_out(md_job *job, md_ctx *ctx, const md_pose *poses, int n);
 
 /* Job properties (valid after md_job_create). */
 int md_job_dims(const md_job *job, int *ng1, int *nf1, int *na_rec, int *na_lig, int *n_rot, int *t,

@@ -271,25 +271,28 @@ int md_job_run(md_job *job, md_ctx *ctx) {
     const int nrot = job->p.num_rot(), t = job->p.num_sort;
     std::vector<float> rot((size_t)nrot * 9);
     for (int r = 0; r < nrot; ++r) rotation_matrix(&job->p.angles[3 * (size_t)r], &rot[9 * (size_t)r]);
-    job->poses.assign((size_t)nrot * t, md_pose{});
-    if ((rc = md_dock(ctx, rot.data(), 0, nrot, t, job->poses.data()))) return fail(rc);
+    std::vector<md_pose> poses((size_t)nrot * t, md_pose{});
+    if ((rc = md_dock(ctx, rot.data(), 0, nrot, t, poses.data()))) return fail(rc);
+    rc = md_job_write_out(job, ctx, poses.data(), (int)poses.size());
+    if (own) md_ctx_destroy(own);
+    return rc;
+}
+
+int md_job_write_out(md_job *job, md_ctx *ctx, const md_pose *poses, int n) {
+    if (!job || (n > 0 && !poses) || n != job->p.num_rot() * job->p.num_sort) {
+        if (job) job->err = "md_job_write_out needs n_rot * t poses";
+        return MD_ERR_ARG;
+    }
+    job->poses.assign(poses, poses + n);
     // FFTProcess::sort_index + Docking::output
     job->top = job->poses;
     md_sort_poses(job->top.data(), (int)job->top.size(), job->p.num_output);
     job->top.resize(std::min((size_t)job->p.num_output, job->top.size()));
-    if (job->p.detail_output && (rc = write_detail(job, ctx))) {
-        if (own) md_ctx_destroy(own);
-        return rc;
-    }
+    int rc;
+    if (job->p.detail_output && ctx && (rc = write_detail(job, ctx))) return rc;
     std::vector<PoseRec> recs;
     for (const md_pose &q : job->top) recs.push_back(PoseRec{q.score, q.rot, q.i, q.j, q.k});
-    if ((rc = write_out_file(job->p.out_file, job->nf1, job->p.grid_width, job->rec, job->lig, job->p, recs,
-                             job->err))) {
-        if (own) md_ctx_destroy(own);
-        return rc;
-    }
-    if (own) md_ctx_destroy(own);
-    return MD_OK;
+    return write_out_file(job->p.out_file, job->nf1, job->p.grid_width, job->rec, job->lig, job->p, recs, job->err);
 }
 
 int md_job_dims(const md_job *job, int *ng1, int *nf1, int *na_rec, int *na_lig, int *n_rot, int *t, int *n_out) {

@@ -288,6 +288,13 @@ class Job:
         if rc:
             raise MdError(rc, N.lib().md_job_error(self._h).decode())
 
+    def write_out(self, poses, fft: FFTProcess | None = None):
+        """Merge n_rot * t poses (rotation-major) and write the .out file."""
+        p = np.ascontiguousarray(poses).view(POSE_DTYPE).reshape(-1)
+        rc = N.lib().md_job_write_out(self._h, fft._h if fft else None, N.vptr(p), len(p))
+        if rc:
+            raise MdError(rc, N.lib().md_job_error(self._h).decode())
+
     def poses(self):
         out = np.zeros(self.n_rot * self.t, POSE_DTYPE)
         N.lib().md_job_poses(self._h, N.vptr(out))
