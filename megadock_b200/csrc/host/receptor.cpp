@@ -100,16 +100,16 @@ void receptor_grids(const Molecule &rec, const Params &p, const std::vector<floa
         const int reach = (int)((12 + gw - 0.01) / gw);
         for (int l = 0; l < na; ++l) {
             const float rd = rec.radius[l] + 3.6f;
-            const float judge2 = rd * rd;
+            const float shell2 = rd * rd;
             const double term = 1.0 + rec.ace[l] * (-0.8) * p.ace_ratio;
             const int i0 = origin(xyz[3 * l]), j0 = origin(xyz[3 * l + 1]), k0 = origin(xyz[3 * l + 2]);
             const float *ax = &dx[(size_t)l * ng1], *ay = &dy[(size_t)l * ng1], *az = &dz[(size_t)l * ng1];
             for (int i = std::max(i0 - reach, 0); i < std::min(i0 + reach + 1, ng1); ++i) {
-                if (ax[i] > judge2) continue;
+                if (ax[i] > shell2) continue;
                 for (int j = std::max(j0 - reach, 0); j < std::min(j0 + reach + 1, ng1); ++j) {
-                    if (ax[i] + ay[j] > judge2) continue;
+                    if (ax[i] + ay[j] > shell2) continue;
                     for (int k = std::max(k0 - reach, 0); k < std::min(k0 + reach + 1, ng1); ++k) {
-                        if (ax[i] + ay[j] + az[k] < judge2) {
+                        if (ax[i] + ay[j] + az[k] < shell2) {
                             float &v = shell[(size_t)ng2 * i + ng1 * j + k];
                             v = (float)(v + term);
                         }

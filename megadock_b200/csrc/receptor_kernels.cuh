@@ -37,7 +37,7 @@ struct RecAtom {
     float x, y, z;
     int io, jo, ko;       // centre cell, (int)(c / gw + ng/2)
     int iw, jw, kw;       // centre cell of the field, (int)(c / width + ng/2)
-    float core2, judge2;  // 1.5 R^2 and (R + 3.6)^2
+    float core2, shell2;  // 1.5 R^2 and (R + 3.6)^2
     double term;          // 1 + ACE (-0.8) ratio
     float q;
     int reach_e;          // field cube half width (-1: uncharged)
@@ -73,7 +73,7 @@ __global__ void k_rec_prep(RecParams P, const float *__restrict__ xyz, const flo
     const float r = radius[l];
     a.core2 = __fmul_rn(__fmul_rn(r, r), 1.5f);
     const float rd = __fadd_rn(r, 3.6f);
-    a.judge2 = __fmul_rn(rd, rd);
+    a.shell2 = __fmul_rn(rd, rd);
     a.term = __dadd_rn(1.0, __dmul_rn(__dmul_rn((double)ace[l], -0.8), P.ace_ratio));
     const float q = charge[l];
     const float aq = fabsf(q);
@@ -226,7 +226,7 @@ __global__ void k_rec_rows(RecParams P, const RecAtom *__restrict__ A, const flo
     for (int l = 0; l < P.na; ++l) {
         const RecAtom &a = A[l];
         if (i < a.io - R || i > a.io + R || j < a.jo - R || j > a.jo + R) continue;
-        if (__fadd_rn(rec_sq(a.x, gc[i]), rec_sq(a.y, gc[j])) > a.judge2) continue;
+        if (__fadd_rn(rec_sq(a.x, gc[i]), rec_sq(a.y, gc[j])) > a.shell2) continue;
         if (out) out[base + n] = l;
         ++n;
     }
@@ -246,7 +246,7 @@ __global__ void k_rec_shell(RecParams P, const RecAtom *__restrict__ A, const fl
         const RecAtom &a = A[list[e]];
         if (k < a.ko - R || k > a.ko + R) continue;
         const float d = __fadd_rn(__fadd_rn(rec_sq(a.x, gc[i]), rec_sq(a.y, gc[j])), rec_sq(a.z, gc[k]));
-        if (d < a.judge2) v = __double2float_rn(__dadd_rn((double)v, a.term));
+        if (d < a.shell2) v = __double2float_rn(__dadd_rn((double)v, a.term));
     }
     if (grid[c] != P.eps_core) grid[c] = v;
 }
