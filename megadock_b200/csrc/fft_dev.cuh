@@ -84,6 +84,35 @@ __device__ __forceinline__ void static_for(F &&f) {
     }
 }
 
+// a * exp(S * 2 pi i e / R) for a compile-time twiddle: quarter turns are
+// swaps and sign flips, odd eighth turns one add pair and a scale by sqrt(1/2),
+// the rest a complex multiply by constexpr cos / sin.
+template <long E, int R, int S>
+__device__ __forceinline__ float2 tw_mul(float2 a) {
+    constexpr long e = ((E % R) + R) % R;
+    if constexpr (e == 0) {
+        return a;
+    } else if constexpr ((4 * e) % R == 0) {
+        constexpr int q = (int)(4 * e / R);   // 1, 2 or 3 quarter turns
+        if constexpr (q == 2) return make_float2(-a.x, -a.y);
+        else if constexpr ((q == 1) == (S > 0)) return make_float2(-a.y, a.x);   // times +i
+        else return make_float2(a.y, -a.x);                                      // times -i
+    } else if constexpr ((8 * e) % R == 0) {
+        constexpr int o = (int)(8 * e / R);   // 1, 3, 5 or 7 eighth turns
+        constexpr float h = 0.70710678118654752f;
+        constexpr float c = (o == 1 || o == 7) ? 1.f : -1.f;                  // sign of cos
+        constexpr float sn = (float)S * ((o == 1 || o == 3) ? 1.f : -1.f);    // sign of S sin
+        // (a.x c - a.y s, a.x s + a.y c) with |c| = |s| = sqrt(1/2)
+        const float re = c > 0 ? (sn > 0 ? a.x - a.y : a.x + a.y) : (sn > 0 ? -a.x - a.y : a.y - a.x);
+        const float im = sn > 0 ? (c > 0 ? a.x + a.y : a.x - a.y) : (c > 0 ? a.y - a.x : -a.x - a.y);
+        return make_float2(re * h, im * h);
+    } else {
+        constexpr float c = ct::cos2pi(e, R);
+        constexpr float s = (float)S * ct::sin2pi(e, R);
+        return make_float2(a.x * c - a.y * s, a.x * s + a.y * c);
+    }
+}
+
 // ------------------------------------------------------------------ small DFTs
 // In-place R-point DFT of v[0..R) with exponent sign S (-1 forward, +1 inverse):
 //   v[k] <- sum_n v[n] * exp(S * 2*pi*i*n*k/R)
@@ -171,14 +200,7 @@ struct Dft {
             Dft<A, S>::run(a);
             static_for<0, A>([&](auto k1_) {
                 constexpr int k1 = decltype(k1_)::value;
-                constexpr long e = (long)n2 * k1;
-                if constexpr (e % R == 0) {
-                    tmp[k1 * B + n2] = a[k1];
-                } else {
-                    constexpr float c = ct::cos2pi(e, R);
-                    constexpr float s = (float)S * ct::sin2pi(e, R);
-                    tmp[k1 * B + n2] = make_float2(a[k1].x * c - a[k1].y * s, a[k1].x * s + a[k1].y * c);
-                }
+                tmp[k1 * B + n2] = tw_mul<(long)n2 * k1, R, S>(a[k1]);
             });
         });
         static_for<0, A>([&](auto k1_) {
