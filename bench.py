@@ -182,6 +182,42 @@ def run_profile_case(args):
     print("profile case done")
 
 
+def run_profile_aux(args):
+    """One small invocation of every auxiliary device path for ncu: receptor
+    grids on the device (N=128 bench pair), the LSE adjoint with ligand-grid
+    gradients, pose scores and the detail score terms (N=96, 150/70 pair)."""
+    import numpy as np
+    import torch
+
+    from megadock_b200 import FFTProcess, Job, POSE_DTYPE, rotation_matrices, synth
+    with tempfile.TemporaryDirectory() as tmp:
+        rp, lp = make_inputs(tmp)
+        job = Job(["-R", rp, "-L", lp, "-F", str(N_FFT), "-r", "24"])
+        fp = FFTProcess(0)
+        fp.alloc_array(job.nf1, job.grid_width, job.grid_coord())
+        xyz, rad, q, ace = job.receptor_atoms()
+        rc, _ = job.centers()
+        fp.receptor_build((xyz - np.asarray(rc, np.float32)).astype(np.float32), rad, q, ace)
+        fp.fft_memory_free()
+        rp, lp = synth.write_pair(tmp, 150, 70, 0, stem="aux")
+        job = Job(["-R", rp, "-L", lp, "-F", "96", "-r", "360", "-O", "-N", "200", "-o", os.path.join(tmp, "a.out")])
+        fp = FFTProcess(0)
+        fp.alloc_array(job.nf1, job.grid_width, job.grid_coord())
+        rr, ri = job.receptor_grids()
+        fp.receptor_fft(rr, ri)
+        x2, r2, q2 = job.ligand_atoms()
+        fp.ligand_data_transfer_gpu(x2, r2, q2, job.lig_core)
+        fp.set_batch(64)
+        mats = rotation_matrices(job.rotation_angles())
+        top1 = fp.cuda_fft(mats, t=1).copy()
+        fp.adjoint_lse(mats, top1, 10.0, 1.0, lig_rot=[int(np.argmax(top1["score"]))])
+        fp.pose_scores(mats[:64], top1[:64])
+        job.run(fp)                       # -O: the detail score terms
+        torch.cuda.synchronize()
+        fp.fft_memory_free()
+    print("profile aux done")
+
+
 def run_pairs_workload(args):
     """64 synthetic pairs, chain lengths log-uniform in 60-800 residues, each
     docked over 3,600 rotations (t=1) in one captured graph: rotation
@@ -356,11 +392,15 @@ def main():
     ap.add_argument("--fit-pairs", type=int, default=32)
     ap.add_argument("--profile-case", type=int, default=0, metavar="R",
                     help="run R rotations of the batched form once (for ncu captures) and exit")
+    ap.add_argument("--profile-aux", action="store_true",
+                    help="one small run of the receptor-grid, adjoint, pose-score and detail kernels (for ncu)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
     if args.profile_case:
         return run_profile_case(args)
+    if args.profile_aux:
+        return run_profile_aux(args)
     if args.workload == "pairs":
         return run_pairs_workload(args)
     if args.workload == "adjoint":
