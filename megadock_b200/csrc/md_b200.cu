@@ -624,11 +624,11 @@ int md_receptor_build(md_ctx *ctx, int na, const float *xyz_centred, const float
         for (int sweep = 0; sweep < 2; ++sweep) k_rec_sweep<<<1, 1024, sweep_smem, s>>>(P, d_r, open_space);
         k_rec_final<<<cells_blocks, 256, 0, s>>>(P, d_r, open_space);
         // surface shell over per-row atom lists
-        k_rec_rows<<<(rows + 127) / 128, 128, 0, s>>>(P, d_atoms, ctx->d_gc, d_cnt, nullptr, nullptr);
+        k_rec_rows<<<(rows + 3) / 4, 128, 0, s>>>(P, d_atoms, ctx->d_gc, d_cnt, nullptr, nullptr);
         const int nlist = scan(rows);
         step(cudaMalloc(&d_list, sizeof(int) * std::max(1, nlist)));
         if (e == cudaSuccess) {
-            k_rec_rows<<<(rows + 127) / 128, 128, 0, s>>>(P, d_atoms, ctx->d_gc, d_cnt, d_start, d_list);
+            k_rec_rows<<<(rows + 3) / 4, 128, 0, s>>>(P, d_atoms, ctx->d_gc, d_cnt, d_start, d_list);
             k_rec_shell<<<cells_blocks, 256, 0, s>>>(P, d_atoms, ctx->d_gc, d_start, d_list, d_r);
             step(cudaGetLastError());
             step(cudaStreamSynchronize(s));
@@ -637,12 +637,12 @@ int md_receptor_build(md_ctx *ctx, int na, const float *xyz_centred, const float
         }
         // electrostatics over per-plane charged-atom lists
         if (e == cudaSuccess) {
-            k_rec_planes<<<(ng + 63) / 64, 64, 0, s>>>(P, d_atoms, d_cnt, nullptr, nullptr);
+            k_rec_planes<<<(ng + 3) / 4, 128, 0, s>>>(P, d_atoms, d_cnt, nullptr, nullptr);
             const int nplane = scan(ng);
             step(cudaMalloc(&d_list, sizeof(int) * std::max(1, nplane)));
         }
         if (e == cudaSuccess) {
-            k_rec_planes<<<(ng + 63) / 64, 64, 0, s>>>(P, d_atoms, d_cnt, d_start, d_list);
+            k_rec_planes<<<(ng + 3) / 4, 128, 0, s>>>(P, d_atoms, d_cnt, d_start, d_list);
             k_rec_elec<<<cells_blocks, 256, 0, s>>>(P, d_atoms, ctx->d_gc, d_start, d_list, d_r, d_i);
             if (make_receptor) launch_receptor(ctx, d_r, d_i);
             step(cudaGetLastError());

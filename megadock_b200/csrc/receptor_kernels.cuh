@@ -171,13 +171,31 @@ __global__ void __launch_bounds__(1024) k_rec_sweep(RecParams P, float *__restri
                     In.w[1] |= q.w[1];
                 }
                 const bool vr = vrow(i, j);
+                // Vk: positions 2 <= k <= ng - 2 (as a source on the k axis)
+                RowMask Vk{{0, 0}};
+#pragma unroll
+                for (int w = 0; w < 2; ++w) {
+                    const int lo = max(2 - 64 * w, 0), hi = min(ng - 2 - 64 * w, 63);   // bit range in word w
+                    if (hi >= lo)
+                        Vk.w[w] = ((hi - lo == 63) ? ~0ull : ((1ull << (hi - lo + 1)) - 1ull)) << lo;
+                }
+                // seeds S = O | (Z & In & Vk); k receives from k - 1 when
+                // P(k) = Z(k) & Vk(k - 1) & vr.  R = S | (P & (R << 1)) is a
+                // carry chain: within a run of P, everything from the first
+                // position after a reached cell up to the run's end is reached,
+                // i.e. P & (~(P + B) | B) with B = (R << 1) & P restricted to
+                // the seeds (the addition carries through the run).
                 RowMask R{{0, 0}};
-                bool prev = false;   // R(k-1) and V(k-1) within this row
-                for (int k = 0; k < ng; ++k) {
-                    const bool vk_in = mbit(In, k) && k >= 2 && k <= ng - 2;   // predecessor on the same k is valid
-                    const bool r = mbit(O, k) || (mbit(Z, k) && (vk_in || prev));
-                    if (r) R.w[k >> 6] |= 1ull << (k & 63);
-                    prev = r && vr && k >= 2 && k <= ng - 2;
+                unsigned long long carry = 0ull;   // R at bit 63 of the previous word
+#pragma unroll
+                for (int w = 0; w < 2; ++w) {
+                    const unsigned long long S = O.w[w] | (Z.w[w] & In.w[w] & Vk.w[w]);
+                    const unsigned long long vprev = (Vk.w[w] << 1) | (w ? (Vk.w[w - 1] >> 63) : 0ull);
+                    const unsigned long long P = vr ? (Z.w[w] & vprev) : 0ull;
+                    const unsigned long long B = ((S << 1) | carry) & P;
+                    const unsigned long long r = S | (P & (~(P + B) | B));
+                    R.w[w] = r;
+                    carry = r >> 63;
                 }
                 Rm[(size_t)i * ng + j] = R;
             }
@@ -213,24 +231,32 @@ __global__ void k_rec_final(RecParams P, float *__restrict__ grid, float open_sp
     }
 }
 
-// Atoms (in order) whose shell cube and sphere reach row (i, j).  count pass
+// Atoms (in order) whose shell cube and sphere reach row (i, j): one warp per
+// row, 32 atoms per step, compacted in order with a ballot.  count pass
 // (out == nullptr) writes cnt[row]; fill pass writes out[start[row] ..].
 __global__ void k_rec_rows(RecParams P, const RecAtom *__restrict__ A, const float *__restrict__ gc,
                            int *__restrict__ cnt, const int *__restrict__ start, int *__restrict__ out) {
-    const int row = blockIdx.x * blockDim.x + threadIdx.x;
+    const int row = (int)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
     const int ng = P.ng;
-    if (row >= ng * ng) return;
+    if (row >= ng * ng) return;   // whole warps
     const int i = row / ng, j = row % ng;
     const int R = P.reach_shell;
-    int n = 0, base = out ? start[row] : 0;
-    for (int l = 0; l < P.na; ++l) {
-        const RecAtom &a = A[l];
-        if (i < a.io - R || i > a.io + R || j < a.jo - R || j > a.jo + R) continue;
-        if (__fadd_rn(rec_sq(a.x, gc[i]), rec_sq(a.y, gc[j])) > a.shell2) continue;
-        if (out) out[base + n] = l;
-        ++n;
+    int n = 0;
+    const int base = out ? start[row] : 0;
+    for (int l0 = 0; l0 < P.na; l0 += 32) {
+        const int l = l0 + lane;
+        bool hit = false;
+        if (l < P.na) {
+            const RecAtom &a = A[l];
+            hit = !(i < a.io - R || i > a.io + R || j < a.jo - R || j > a.jo + R) &&
+                  !(__fadd_rn(rec_sq(a.x, gc[i]), rec_sq(a.y, gc[j])) > a.shell2);
+        }
+        const unsigned m = __ballot_sync(0xffffffffu, hit);
+        if (hit && out) out[base + n + __popc(m & ((1u << lane) - 1u))] = l;
+        n += __popc(m);
     }
-    if (!out) cnt[row] = n;
+    if (!out && lane == 0) cnt[row] = n;
 }
 
 __global__ void k_rec_shell(RecParams P, const RecAtom *__restrict__ A, const float *__restrict__ gc,
@@ -251,19 +277,26 @@ __global__ void k_rec_shell(RecParams P, const RecAtom *__restrict__ A, const fl
     if (grid[c] != P.eps_core) grid[c] = v;
 }
 
-// Charged atoms (in order) whose field cube reaches plane i.
+// Charged atoms (in order) whose field cube reaches plane i: one warp per plane.
 __global__ void k_rec_planes(RecParams P, const RecAtom *__restrict__ A, int *__restrict__ cnt,
                              const int *__restrict__ start, int *__restrict__ out) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= P.ng) return;
-    int n = 0, base = out ? start[i] : 0;
-    for (int l = 0; l < P.na; ++l) {
-        const RecAtom &a = A[l];
-        if (a.reach_e < 0 || i < a.iw - a.reach_e || i > a.iw + a.reach_e) continue;
-        if (out) out[base + n] = l;
-        ++n;
+    const int i = (int)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    if (i >= P.ng) return;   // whole warps
+    int n = 0;
+    const int base = out ? start[i] : 0;
+    for (int l0 = 0; l0 < P.na; l0 += 32) {
+        const int l = l0 + lane;
+        bool hit = false;
+        if (l < P.na) {
+            const RecAtom &a = A[l];
+            hit = a.reach_e >= 0 && i >= a.iw - a.reach_e && i <= a.iw + a.reach_e;
+        }
+        const unsigned m = __ballot_sync(0xffffffffu, hit);
+        if (hit && out) out[base + n + __popc(m & ((1u << lane) - 1u))] = l;
+        n += __popc(m);
     }
-    if (!out) cnt[i] = n;
+    if (!out && lane == 0) cnt[i] = n;
 }
 
 __global__ void k_rec_elec(RecParams P, const RecAtom *__restrict__ A, const float *__restrict__ gc,
