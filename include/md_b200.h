@@ -210,6 +210,10 @@ void md_job_destroy(md_job *job);
 /* Control::execute (src/control.cpp:468-529): dock every rotation on ctx and
  * write the .out file.  ctx may be NULL (a context on device 0 is made). */
 int md_job_run(md_job *job, md_ctx *ctx);
+/* The job's receptor grids built on the device (md_receptor_build with the
+ * job's atoms and -a/-d/-e values) and made ctx's receptor; ctx must have the
+ * job's grid (md_set_grid with nf1, grid width and grid coordinates). */
+int md_job_receptor_to(const md_job *job, md_ctx *ctx);
 /* The output half of md_job_run for poses docked elsewhere (for example
  * gathered from several GPUs): the n = n_rot * t poses in rotation-major
  * order are merged (FFTProcess::sort_index, src/fft_process.cpp:469-479) and

@@ -70,6 +70,7 @@ _PROTOS = {
     "md_job_log": (_CP, [_VP]),
     "md_job_destroy": (None, [_VP]),
     "md_job_run": (C.c_int, [_VP, _VP]),
+    "md_job_receptor_to": (C.c_int, [_VP, _VP]),
     "md_job_write_out": (C.c_int, [_VP, _VP, _VP, C.c_int]),
     "md_job_dims": (C.c_int, [_VP, _IP, _IP, _IP, _IP, _IP, _IP, _IP]),
     "md_job_grid_width": (C.c_float, [_VP]),

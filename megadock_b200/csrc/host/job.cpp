@@ -239,6 +239,14 @@ int write_detail(md_job *job, md_ctx *ctx) {
 
 extern "C" {
 
+int md_job_receptor_to(const md_job *job, md_ctx *ctx) {
+    if (!job || !ctx) return MD_ERR_ARG;
+    const std::vector<float> xyz = centred_coordinates(job->rec);
+    return md_receptor_build(ctx, job->rec.na(), xyz.data(), job->rec.radius.data(), job->rec.charge.data(),
+                             job->rec.ace.data(), job->p.rec_core, job->p.ace_ratio, job->p.elec_ratio, 1, nullptr,
+                             nullptr);
+}
+
 int md_job_run(md_job *job, md_ctx *ctx) {
     if (!job) return MD_ERR_ARG;
     md_ctx *own = nullptr;
@@ -257,14 +265,7 @@ int md_job_run(md_job *job, md_ctx *ctx) {
     };
     int rc;
     if ((rc = md_set_grid(ctx, job->nf1, job->p.grid_width, job->gc.data()))) return fail(rc);
-    {
-        // receptor grids and R^ on the device
-        const std::vector<float> xyz = centred_coordinates(job->rec);
-        if ((rc = md_receptor_build(ctx, job->rec.na(), xyz.data(), job->rec.radius.data(), job->rec.charge.data(),
-                                    job->rec.ace.data(), job->p.rec_core, job->p.ace_ratio, job->p.elec_ratio, 1,
-                                    nullptr, nullptr)))
-            return fail(rc);
-    }
+    if ((rc = md_job_receptor_to(job, ctx))) return fail(rc);   // receptor grids and R^ on the device
     if ((rc = md_ligand_data(ctx, job->lig.na(), job->lig_xyz.data(), job->lig.radius.data(),
                              job->lig.charge.data(), job->p.lig_core)))
         return fail(rc);

@@ -288,6 +288,13 @@ class Job:
         if rc:
             raise MdError(rc, N.lib().md_job_error(self._h).decode())
 
+    def receptor_to(self, fft: FFTProcess):
+        """Build this job's receptor grids on fft's device and make them its
+        receptor (fft must hold this job's grid: alloc_array(nf1, ...))."""
+        rc = N.lib().md_job_receptor_to(self._h, fft._h)
+        if rc:
+            raise MdError(rc, N.lib().md_last_error(fft._h).decode())
+
     def write_out(self, poses, fft: FFTProcess | None = None):
         """Merge n_rot * t poses (rotation-major) and write the .out file."""
         p = np.ascontiguousarray(poses).view(POSE_DTYPE).reshape(-1)

@@ -83,8 +83,7 @@ class PairBatch:
                         nf += 4
             fp = FFTProcess(device)
             fp.alloc_array(job.nf1, job.grid_width, job.grid_coord())
-            rr, ri = job.receptor_grids()
-            fp.receptor_fft(rr, ri)
+            job.receptor_to(fp)
             xyz, rad, q = job.ligand_atoms()
             fp.ligand_data_transfer_gpu(xyz, rad, q, job.lig_core)
             self.jobs.append(job)
