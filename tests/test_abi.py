@@ -35,3 +35,23 @@ def test_kernel_sizes_built(built):
         assert lib().md_fft_size_supported(n) == 1
     for n in (90, 98, 2048):
         assert lib().md_fft_size_supported(n) == 0
+
+
+def test_null_arguments_are_rejected(built):
+    """Entry points check their pointers before touching a device (no GPU needed)."""
+    import ctypes as C
+
+    from megadock_b200 import _native as N
+    L = N.lib()
+    E = N.MD_ERR_ARG
+    f = C.POINTER(C.c_float)()
+    assert L.md_adjoint_lse(None, f, 1, None, 10.0, 1.0, None, f, f, f, None, None, 0, f, f) == E
+    assert L.md_adjoint_poses(None, f, 1, None, f, f, f, f, None, 0, f, f) == E
+    assert L.md_pose_scores(None, f, 1, None, f) == E
+    assert L.md_pose_terms(None, f, f, 1, None, f) == E
+    assert L.md_receptor_build(None, 1, f, f, f, f, -45.0, 1.0, 1.0, 1, f, f) == E
+    assert L.md_job_receptor_to(None, None) == E
+    assert L.md_job_write_out(None, None, None, 0) == E
+    assert L.md_decoy_pdb(None, None, 1, None) == E
+    assert L.md_ligand_centres(None, 0, None) == E
+    assert L.md_decoy_pdb(b"/nonexistent.out", b"/nonexistent.pdb", 1, b"/tmp/x.pdb") == N.MD_ERR_IO
