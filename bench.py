@@ -251,7 +251,8 @@ def run_pairs_workload(args):
         "dtype": "f32", "data": "synthetic",
         "config": {"workload": "64 synthetic pairs, chains log-uniform 60-800 residues, t=1",
                    "fft_sizes": {str(k): v for k, v in sorted(sizes.items())},
-                   "rotations_per_launch": {str(k): v for k, v in sorted(pb.batch_by_n.items())}},
+                   "rotations_per_launch": {str(k): v for k, v in sorted(pb.batch_by_n.items())},
+                   "inverse_plane_plan": {str(k): v for k, v in sorted(pb.plan_by_n.items())}},
         "pairs_per_s": len(pb.ctxs) / (ms * 1e-3),
         "clocks": clk.summary(),
     }
@@ -383,7 +384,8 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--batch", type=int, default=0, help="rotations per launch (0 = autotune)")
+    ap.add_argument("--batch", type=int, default=0, help="rotations per launch (0 = autotune batch and plan)")
+    ap.add_argument("--plan", type=int, default=0, help="inverse plane kernel radix plan with --batch (0, 1, 2)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="metric", choices=["metric", "pairs", "adjoint", "fit"],
                     help="metric: the headline workload; pairs: 64 uneven synthetic pairs, 3,600 rotations each; "
@@ -423,7 +425,7 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
 
     from megadock_b200 import FFTProcess, Job, rotation_matrices
-    from megadock_b200.tune import autotune_batch
+    from megadock_b200.tune import autotune
 
     # a dedicated stream: the library captures CUDA graphs on it, which the
     # legacy default stream does not allow
@@ -444,7 +446,11 @@ def main():
         d_rot = torch.from_numpy(mats).to(f"cuda:{local}")
         d_pose = torch.zeros(nrot * T_POSES * 5, dtype=torch.int32, device=f"cuda:{local}")
 
-        batch = args.batch or autotune_batch(fp, d_rot.data_ptr(), d_pose.data_ptr(), T_POSES)
+        if args.batch:
+            batch, plan = args.batch, args.plan
+            fp.set_plan(plan)
+        else:
+            batch, plan = autotune(fp, d_rot.data_ptr(), d_pose.data_ptr(), T_POSES)
 
         def timed(fn, steps, warmup):
             for _ in range(warmup):
@@ -551,6 +557,7 @@ def main():
         "config": {"workload": f"docking, {N_REC}/{N_LIG}-residue synthetic pair ({job.na_rec}/{job.na_lig} atoms), "
                                f"N={N_FFT}, {ROT_SET} rotations, t={T_POSES}",
                    "fft": N_FFT, "rotations": ROT_SET, "t": T_POSES, "rotations_per_launch": batch,
+                   "inverse_plane_plan": plan,
                    "l2": "working set per step >> L2 (54,000 rotations x ~25 MB of intermediates)",
                    "parallelism": f"replicas x{world}"},
         "plain": {"value": plain, "ms_per_step": ms_plain, "unit": "rotations/s",

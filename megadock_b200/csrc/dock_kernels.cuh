@@ -765,19 +765,32 @@ struct TopList {
 // this plane's candidates cand[(b*N + x)*t + out0 + j] for j < nsel.
 // Keys are raw scores: ordering by raw equals ordering by raw / nf3 (a
 // positive constant), so the merge kernel divides only the winners.
-// Three CTAs per SM (<= 42 registers) where the radices are small enough.
-template <int N, int T>
+// Radix plans of this kernel, chosen per context by the autotuner: variant 0
+// uses the line plans of N (kz) and N/2 (ky), variant 1 reverses the kz split
+// (R2 x R1), variant 2 the ky split.  Three CTAs per SM (<= 42 registers)
+// where the radices are small enough.
+constexpr int kC2RPlans = 3;
+template <int N, int V>
+struct C2RPlan {
+    static constexpr int R1 = V == 1 ? Plan<N>::R2 : Plan<N>::R1;
+    static constexpr int R2 = V == 1 ? Plan<N>::R1 : Plan<N>::R2;
+    static constexpr int Q1 = V == 2 ? Plan<N / 2>::R2 : Plan<N / 2>::R1;
+    static constexpr int Q2 = V == 2 ? Plan<N / 2>::R1 : Plan<N / 2>::R2;
+};
+
+template <int N, int T, int V = 0>
 constexpr int c2r_min_blocks() {
-    return (T <= 4 && Plan<N>::R1 <= 8 && Plan<N>::R2 <= 16 && Plan<N / 2>::R1 <= 8 && Plan<N / 2>::R2 <= 16) ? 3 : 2;
+    using P = C2RPlan<N, V>;
+    return (T <= 4 && P::R1 <= 8 && P::R2 <= 16 && P::Q1 <= 8 && P::Q2 <= 16) ? 3 : 2;
 }
 
-template <int N, int T>
-__global__ void __launch_bounds__(kNT, c2r_min_blocks<N, T>())
+template <int N, int T, int V = 0>
+__global__ void __launch_bounds__(kNT, c2r_min_blocks<N, T, V>())
     k_plane_c2r(GridView G, const float2 *__restrict__ Gh, int t, float nf3f, int out0, int nsel,
                 Cand *__restrict__ cand) {
     constexpr int NH = N / 2;
-    constexpr int R1 = Plan<N>::R1, R2 = Plan<N>::R2;
-    constexpr int Q1 = Plan<NH>::R1, Q2 = Plan<NH>::R2;
+    constexpr int R1 = C2RPlan<N, V>::R1, R2 = C2RPlan<N, V>::R2;
+    constexpr int Q1 = C2RPlan<N, V>::Q1, Q2 = C2RPlan<N, V>::Q2;
     constexpr int PA = N + N / R2;   // step-1 layout: one pad per R2 block
     constexpr int PB = N + 8;        // step-2 layout (natural order)
     constexpr int PITCH = PA > PB ? PA : PB;

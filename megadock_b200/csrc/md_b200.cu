@@ -104,6 +104,7 @@ struct md_ctx {
     bool have_ligand = false;
     // work sets (lane 0 serves every form; lane 1 the batched graph)
     int batch = 1;
+    int plan = 0;   // radix plan variant of the plane top-t kernel (C2RPlan)
     int cap = 0, cap_t = 0, cap_na = 0;
     WorkSet::Sizes have{};           // bytes held by each work-set buffer
     WorkSet ws[kLanes];
@@ -139,8 +140,9 @@ struct Sized {
     static constexpr int TILES = (N + kLT - 1) / kLT;
     static size_t smem_fwd() { return (size_t)N * (N + 1) * sizeof(float2); }
     static size_t smem_xline() { return (size_t)2 * N * kLT * sizeof(float2); }
+    template <int V = 0>
     static size_t smem_c2r() {
-        constexpr int PA = N + Plan<N>::R1, PB = N + 8;
+        constexpr int PA = N + C2RPlan<N, V>::R1, PB = N + 8;
         return (size_t)NH * (PA > PB ? PA : PB) * sizeof(float2);
     }
 
@@ -155,9 +157,13 @@ struct Sized {
         set((const void *)k_plane_fwd<N, 1>, smem_fwd());
         set((const void *)k_plane_fwd<N, 2>, smem_fwd());
         set((const void *)k_xline_herm<N>, smem_xline());
-        set((const void *)k_plane_c2r<N, 1>, smem_c2r());
-        set((const void *)k_plane_c2r<N, 4>, smem_c2r());
-        set((const void *)k_plane_c2r<N, 16>, smem_c2r());
+        set((const void *)k_plane_c2r<N, 1, 0>, smem_c2r<0>());
+        set((const void *)k_plane_c2r<N, 4, 0>, smem_c2r<0>());
+        set((const void *)k_plane_c2r<N, 16, 0>, smem_c2r<0>());
+        set((const void *)k_plane_c2r<N, 1, 1>, smem_c2r<1>());
+        set((const void *)k_plane_c2r<N, 4, 1>, smem_c2r<1>());
+        set((const void *)k_plane_c2r<N, 1, 2>, smem_c2r<2>());
+        set((const void *)k_plane_c2r<N, 4, 2>, smem_c2r<2>());
         if (e == cudaSuccess) done = true;
         return e;
     }
@@ -198,17 +204,29 @@ struct Sized {
                                                                         nullptr, nullptr, d_vr, d_vi);
     }
 
-    // The plane top-t kernel in passes of T candidates (T = 1, 4 or 16).
-    static void plane_topt(cudaStream_t s, const GridView &G, const float2 *Gh, int nb, int t, float nf3f, Cand *cand) {
+    // The plane top-t kernel in passes of T candidates (T = 1, 4 or 16), with
+    // radix plan variant `plan` (T = 16 always uses variant 0).
+    template <int T, int V>
+    static void c2r(cudaStream_t s, const GridView &G, const float2 *Gh, int nb, int t, float nf3f, int out0,
+                    int nsel, Cand *cand) {
+        k_plane_c2r<N, T, V><<<dim3(N, nb), kNT, smem_c2r<V>(), s>>>(G, Gh, t, nf3f, out0, nsel, cand);
+    }
+    static void plane_topt(cudaStream_t s, const GridView &G, const float2 *Gh, int nb, int t, float nf3f, Cand *cand,
+                           int plan) {
         const int T = t == 1 ? 1 : (t <= 4 ? 4 : 16);
         for (int out0 = 0; out0 < t; out0 += T) {
             const int nsel = std::min(T, t - out0);
-            if (T == 1)
-                k_plane_c2r<N, 1><<<dim3(N, nb), kNT, smem_c2r(), s>>>(G, Gh, t, nf3f, out0, nsel, cand);
-            else if (T == 4)
-                k_plane_c2r<N, 4><<<dim3(N, nb), kNT, smem_c2r(), s>>>(G, Gh, t, nf3f, out0, nsel, cand);
-            else
-                k_plane_c2r<N, 16><<<dim3(N, nb), kNT, smem_c2r(), s>>>(G, Gh, t, nf3f, out0, nsel, cand);
+            if (T == 1) {
+                if (plan == 1) c2r<1, 1>(s, G, Gh, nb, t, nf3f, out0, nsel, cand);
+                else if (plan == 2) c2r<1, 2>(s, G, Gh, nb, t, nf3f, out0, nsel, cand);
+                else c2r<1, 0>(s, G, Gh, nb, t, nf3f, out0, nsel, cand);
+            } else if (T == 4) {
+                if (plan == 1) c2r<4, 1>(s, G, Gh, nb, t, nf3f, out0, nsel, cand);
+                else if (plan == 2) c2r<4, 2>(s, G, Gh, nb, t, nf3f, out0, nsel, cand);
+                else c2r<4, 0>(s, G, Gh, nb, t, nf3f, out0, nsel, cand);
+            } else {
+                c2r<16, 0>(s, G, Gh, nb, t, nf3f, out0, nsel, cand);
+            }
         }
     }
 
@@ -227,7 +245,7 @@ struct Sized {
         if (ev) cudaEventRecord(ev[2], s);
         k_xline_herm<N><<<dim3(NH * TILES, nb), kNT, smem_xline(), s>>>(G, w.A, c->d_Rh, w.G);
         if (ev) cudaEventRecord(ev[3], s);
-        plane_topt(s, G, w.G, nb, t, nf3f, w.cand);
+        plane_topt(s, G, w.G, nb, t, nf3f, w.cand, c->plan);
         if (ev) cudaEventRecord(ev[4], s);
         k_merge<<<nb, 256, 0, s>>>(w.cand, N, t, N, nf3f, rot0, d_pose);
         if (ev) cudaEventRecord(ev[5], s);
@@ -724,6 +742,15 @@ int md_ligand_data(md_ctx *ctx, int na, const float *xyz, const float *radius, c
 int md_set_batch(md_ctx *ctx, int b) {
     if (!ctx || b < 1) return MD_ERR_ARG;
     ctx->batch = b;
+    return MD_OK;
+}
+
+int md_set_plan(md_ctx *ctx, int plan) {
+    if (!ctx || plan < 0 || plan >= kC2RPlans) return MD_ERR_ARG;
+    if (plan != ctx->plan) {
+        free_graphs(ctx);   // captured launches name the kernels
+        ctx->plan = plan;
+    }
     return MD_OK;
 }
 

@@ -86,6 +86,11 @@ class FFTProcess:
     def set_batch(self, rotations_per_launch: int):
         _check(N.lib().md_set_batch(self._h, int(rotations_per_launch)), self._h)
 
+    def set_plan(self, plan: int):
+        """Radix plan variant of the inverse plane kernel (0, 1 or 2)."""
+        _check(N.lib().md_set_plan(self._h, int(plan)), self._h)
+        self.plan = int(plan)
+
     # -- FFTProcess::cuda_fft over a rotation range
     def cuda_fft(self, rotmats: np.ndarray, t: int = 1, first_rot: int = 0) -> np.ndarray:
         m = np.ascontiguousarray(rotmats, dtype=np.float32).reshape(-1, 9)

@@ -4,8 +4,10 @@ MEGADOCK docks one pair per process and farms pairs out with MPI
 (src/mpidp.cpp:281-551).  Here every pair gets a device context (its receptor
 spectrum and ligand stay resident) and one captured CUDA graph runs the
 rotations of all pairs back to back on a runner context's shared work
-buffers (md_dock_pairs).  Rotations per launch are chosen per FFT size by the
-autotuner (megadock_b200.tune).
+buffers (md_dock_pairs).
+
+Rotations per launch and the inverse plane kernel's radix plan are chosen per
+FFT size by the autotuner (megadock_b200.tune).
 
 Grid choice: each pair uses the smallest N = 2 * ng with ng a 2^a 3^b 5^c
 number (even, so the zero-padded half is aligned) that covers the complex by
@@ -94,15 +96,16 @@ class PairBatch:
         self.d_rot = torch.from_numpy(mats).to(f"cuda:{device}")
         self.d_out = [torch.zeros(self.n_rot * t * 5, dtype=torch.int32, device=f"cuda:{device}")
                       for _ in self.ctxs]
-        self.batch_by_n = {}
+        self.batch_by_n, self.plan_by_n = {}, {}
         if autotune:
-            from .tune import autotune_batch
+            from .tune import autotune
             for fp in self.ctxs:
                 if fp.num_fft not in self.batch_by_n:
-                    self.batch_by_n[fp.num_fft] = autotune_batch(fp, self.d_rot.data_ptr(), self.d_out[0].data_ptr(),
-                                                                 t, sample=min(768, self.n_rot))
+                    self.batch_by_n[fp.num_fft], self.plan_by_n[fp.num_fft] = autotune(
+                        fp, self.d_rot.data_ptr(), self.d_out[0].data_ptr(), t, sample=min(768, self.n_rot))
         for fp in self.ctxs:
             fp.set_batch(self.batch_by_n.get(fp.num_fft, 16))
+            fp.set_plan(self.plan_by_n.get(fp.num_fft, 0))
         self.runner = FFTProcess(device, stream=stream)
 
     def run(self, stream=None):

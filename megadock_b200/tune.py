@@ -1,30 +1,57 @@
-"""Autotuner for the batched form: rotations per launch.
+"""Autotuner for the batched form: rotations per launch and radix plan.
 
 The batched pipeline's cost per rotation falls as more rotations share a
 launch (fuller grids, fewer launches) until the per-launch intermediates stop
-fitting in L2.  ``autotune_batch`` times a sample of rotations at each
-candidate size with the library's per-stage CUDA events (md_dock_profile) and
-returns the fastest.  Results are cached per (N, t, sample) in-process.
+fitting in L2, and the inverse plane kernel (the largest stage) runs at
+different speeds with different radix splits of its two axes (md_set_plan:
+variant 0 the line plans, 1 the kz split reversed, 2 the ky split reversed),
+depending on the size.  ``autotune`` times a sample of rotations with the
+library's per-stage CUDA events (md_dock_profile): first every batch size with
+plan 0, then every plan at the best batch, and keeps the fastest pair.
+Results are cached per (N, t, sample) in-process.
 """
 from __future__ import annotations
 
 _cache: dict = {}
 
 CANDIDATES = (4, 8, 16, 24, 32, 48, 64)
+PLANS = (0, 1, 2)
+
+
+def _time(fp, d_rotmat, d_out, t, sample, b):
+    fp.set_batch(b)
+    fp.dock_profile(d_rotmat, 0, min(sample, 2 * b), t, d_out)   # allocate + warm
+    ms, _ = fp.dock_profile(d_rotmat, 0, sample, t, d_out)
+    return float(ms.sum())
+
+
+def autotune(fp, d_rotmat: int, d_out: int, t: int, sample: int = 1536, candidates=CANDIDATES,
+             plans=PLANS) -> tuple[int, int]:
+    """(rotations per launch, plan) for context fp, left set on fp."""
+    key = (fp.num_fft, t, sample, tuple(candidates), tuple(plans))
+    if key in _cache:
+        b, p = _cache[key]
+        fp.set_batch(b)
+        fp.set_plan(p)
+        return b, p
+    fp.set_plan(plans[0])
+    best_b, best_ms = candidates[0], float("inf")
+    for b in candidates:
+        ms = _time(fp, d_rotmat, d_out, t, sample, b)
+        if ms < best_ms:
+            best_b, best_ms = b, ms
+    best_p = plans[0]
+    for p in plans[1:]:
+        fp.set_plan(p)
+        ms = _time(fp, d_rotmat, d_out, t, sample, best_b)
+        if ms < best_ms:
+            best_p, best_ms = p, ms
+    fp.set_batch(best_b)
+    fp.set_plan(best_p)
+    _cache[key] = (best_b, best_p)
+    return best_b, best_p
 
 
 def autotune_batch(fp, d_rotmat: int, d_out: int, t: int, sample: int = 1536, candidates=CANDIDATES) -> int:
-    key = (fp.num_fft, t, sample, tuple(candidates))
-    if key in _cache:
-        return _cache[key]
-    best, best_ms = candidates[0], float("inf")
-    for b in candidates:
-        fp.set_batch(b)
-        fp.dock_profile(d_rotmat, 0, min(sample, 2 * b), t, d_out)   # allocate + warm
-        ms, _ = fp.dock_profile(d_rotmat, 0, sample, t, d_out)
-        total = float(ms.sum())
-        if total < best_ms:
-            best, best_ms = b, total
-    fp.set_batch(best)
-    _cache[key] = best
-    return best
+    """Rotations per launch (the plan is tuned and set on fp too)."""
+    return autotune(fp, d_rotmat, d_out, t, sample, candidates)[0]

@@ -198,3 +198,24 @@ def test_errors_are_status_codes(built, gpu):
     with pytest.raises(MdError) as e:
         fp.ligand_data_transfer_gpu(np.zeros((40000, 3)), np.ones(40000), np.zeros(40000))
     assert e.value.code == 4
+
+
+@pytest.mark.parametrize("name,extra,t", [("c0", ("-F", "96", "-r", "360"), 1), ("c1", ("-F", "128", "-r", "360"), 3),
+                                          ("small", ("-F", "100", "-r", "360"), 2),
+                                          ("small", ("-F", "120", "-r", "360"), 4)])
+def test_plan_variants_agree(built, gpu, pairs, name, extra, t):
+    """Every radix plan of the inverse plane kernel gives the plan-0 scores
+    within float rounding and the same cells away from near ties."""
+    from megadock_b200 import rotation_matrices
+    job, fp = _setup(pairs, name, *extra)
+    mats = rotation_matrices(job.rotation_angles())
+    fp.set_batch(32)
+    ref = fp.cuda_fft(mats, t=t).copy()
+    for plan in (1, 2):
+        fp.set_plan(plan)
+        got = fp.cuda_fft(mats, t=t).copy()
+        s0, s1 = ref["score"].astype(np.float64), got["score"].astype(np.float64)
+        assert np.all(np.abs(s1 - s0) <= 1e-5 * np.abs(s0) + 1e-4), plan
+        same = (ref["i"] == got["i"]) & (ref["j"] == got["j"]) & (ref["k"] == got["k"])
+        assert same.mean() >= 0.98, (plan, same.mean())
+    fp.set_plan(0)
