@@ -205,7 +205,8 @@ def test_errors_are_status_codes(built, gpu):
                                           ("small", ("-F", "120", "-r", "360"), 4)])
 def test_plan_variants_agree(built, gpu, pairs, name, extra, t):
     """Every radix plan of the inverse plane kernel gives the plan-0 scores
-    within float rounding and the same cells away from near ties."""
+    within twice the FP64-oracle tolerance (both are FP32 FFTs of the same
+    grids, each within RTOL of FP64) and the same cells away from near ties."""
     from megadock_b200 import rotation_matrices
     job, fp = _setup(pairs, name, *extra)
     mats = rotation_matrices(job.rotation_angles())
@@ -215,7 +216,7 @@ def test_plan_variants_agree(built, gpu, pairs, name, extra, t):
         fp.set_plan(plan)
         got = fp.cuda_fft(mats, t=t).copy()
         s0, s1 = ref["score"].astype(np.float64), got["score"].astype(np.float64)
-        assert np.all(np.abs(s1 - s0) <= 1e-5 * np.abs(s0) + 1e-4), plan
+        assert np.all(np.abs(s1 - s0) <= 2 * (RTOL * np.abs(s0) + ATOL)), plan
         same = (ref["i"] == got["i"]) & (ref["j"] == got["j"]) & (ref["k"] == got["k"])
         assert same.mean() >= 0.98, (plan, same.mean())
     fp.set_plan(0)
