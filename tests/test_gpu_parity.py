@@ -95,15 +95,20 @@ def _check_rotation(got, rhat, job, r, t, m):
     s, idx = O.score_sort(raw, t)
     nf = job.nf1
     nf3 = float(nf ** 3)
+    errs, same = [], 0
     for k in range(t):
         g = got[k]
         assert g["rot"] == r
         assert abs(g["score"] - s[k]) <= RTOL * abs(s[k]) + ATOL, (r, k, g["score"], s[k])
+        errs.append(abs(float(g["score"]) - float(s[k])) / max(abs(float(s[k])), 1e-30))
         gi_ = (g["i"], g["j"], g["k"])
         if tuple(idx[k]) != gi_:
             # near tie: the oracle's score at the device's cell must be as good
             alt = raw[gi_] / nf3
             assert abs(alt - s[k]) <= RTOL * abs(s[k]) + ATOL, (r, k, gi_, tuple(idx[k]), alt, s[k])
+        else:
+            same += 1
+    return errs, same
 
 
 @pytest.mark.parametrize("name,extra,t,nchk", [
@@ -128,10 +133,15 @@ def test_dock_matches_fp64_oracle(built, gpu, pairs, name, extra, t, nchk):
     sel = np.linspace(0, job.n_rot - 1, nchk).astype(int)
     mats = rotation_matrices(ang[sel])
     got = fp.cuda_fft(mats, t=t, first_rot=0)
+    errs, same = [], 0
     for n, r in enumerate(sel):
         g = got[n * t:(n + 1) * t].copy()
         g["rot"] = r
-        _check_rotation(g, rhat, job, r, t, mats[n])
+        e, k = _check_rotation(g, rhat, job, r, t, mats[n])
+        errs += e
+        same += k
+    print(f"\nN={job.nf1} t={t}: {len(errs)} poses, max |device - FP64| / |FP64| = {max(errs):.2e}, "
+          f"median {np.median(errs):.2e}; cell equal to the FP64 argmax for {same} of {len(errs)}")
 
 
 @needs_ref
@@ -143,10 +153,13 @@ def test_dock_matches_reference_fp32(built, gpu, pairs):
     ref = RefSession(_args(pairs, "c0", *args))
     ang = job.rotation_angles()
     got = fp.cuda_fft(rotation_matrices(ang[:8]), t=2)
+    errs = []
     for r in range(8):
         s, idx = ref.dock_rotation(r)
         g = got[2 * r:2 * r + 2]
         np.testing.assert_allclose(g["score"], s, rtol=RTOL, atol=ATOL)
+        errs += list(np.abs(g["score"].astype(np.float64) - s) / np.maximum(np.abs(s), 1e-30))
+    print(f"\nvs the reference's FP32 path (project FFT shim): max relative error {max(errs):.2e}")
 
 
 def test_batched_equals_plain(built, gpu, pairs):
