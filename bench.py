@@ -252,7 +252,8 @@ def run_pairs_workload(args):
         "config": {"workload": "64 synthetic pairs, chains log-uniform 60-800 residues, t=1",
                    "fft_sizes": {str(k): v for k, v in sorted(sizes.items())},
                    "rotations_per_launch": {str(k): v for k, v in sorted(pb.batch_by_n.items())},
-                   "inverse_plane_plan": {str(k): v for k, v in sorted(pb.plan_by_n.items())}},
+                   "inverse_plane_plan": {str(k): v for k, v in sorted(pb.plan_by_n.items())},
+                   "xline_tile": {str(k): v for k, v in sorted(pb.tile_by_n.items())}},
         "pairs_per_s": len(pb.ctxs) / (ms * 1e-3),
         "clocks": clk.summary(),
     }
@@ -386,6 +387,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--batch", type=int, default=0, help="rotations per launch (0 = autotune batch and plan)")
     ap.add_argument("--plan", type=int, default=0, help="inverse plane kernel radix plan with --batch (0, 1, 2)")
+    ap.add_argument("--tile", type=int, default=32, help="x-line kernel kz lines per CTA with --batch (16, 32)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="metric", choices=["metric", "pairs", "adjoint", "fit"],
                     help="metric: the headline workload; pairs: 64 uneven synthetic pairs, 3,600 rotations each; "
@@ -449,8 +451,10 @@ def main():
         if args.batch:
             batch, plan = args.batch, args.plan
             fp.set_plan(plan)
+            fp.set_tile(args.tile)
         else:
             batch, plan = autotune(fp, d_rot.data_ptr(), d_pose.data_ptr(), T_POSES)
+        tile = fp.tile
 
         def timed(fn, steps, warmup):
             for _ in range(warmup):
@@ -557,7 +561,7 @@ def main():
         "config": {"workload": f"docking, {N_REC}/{N_LIG}-residue synthetic pair ({job.na_rec}/{job.na_lig} atoms), "
                                f"N={N_FFT}, {ROT_SET} rotations, t={T_POSES}",
                    "fft": N_FFT, "rotations": ROT_SET, "t": T_POSES, "rotations_per_launch": batch,
-                   "inverse_plane_plan": plan,
+                   "inverse_plane_plan": plan, "xline_tile": tile,
                    "l2": "working set per step >> L2 (54,000 rotations x ~25 MB of intermediates)",
                    "parallelism": f"replicas x{world}"},
         "plain": {"value": plain, "ms_per_step": ms_plain, "unit": "rotations/s",

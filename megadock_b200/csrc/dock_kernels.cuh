@@ -547,19 +547,22 @@ __global__ void __launch_bounds__(kNT)
 // the pruned forward x-FFT, multiplies both by conj(R^), folds the mirror into
 // H and runs the inverse x-FFT of the own tile.  CTAs of row 0 run two passes
 // (ky = 0 and ky = N/2) and pack them.  Output Gh[x][ky][kz], ky < N/2.
-template <int N>
-__global__ void __launch_bounds__(kNT)
+// LT kz lines per CTA (the tile shape the autotuner picks, 16 or 32), 16 LT
+// threads, 2 * 32 / LT CTAs per SM.
+template <int N, int LT = kLT>
+__global__ void __launch_bounds__(16 * LT, 64 / LT)
     k_xline_herm(GridView G, const float2 *__restrict__ A, const float2 *__restrict__ Rh, float2 *__restrict__ Gh) {
     constexpr int NG = N / 2, NH = N / 2, OFF = N / 4;
     constexpr int R1 = Plan<N>::R1, R2 = Plan<N>::R2;
     static_assert(R1 % 4 == 0, "pruned forward x pass needs R1 % 4 == 0");
-    constexpr int TILES = (N + kLT - 1) / kLT;
+    constexpr int TILES = (N + LT - 1) / LT;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    float2 *X0 = reinterpret_cast<float2 *>(smem_raw);   // own tile   [N][kLT]
-    float2 *X1 = X0 + N * kLT;                           // mirror tile [N][kLT]
-    const int lane = threadIdx.x & 31;
+    float2 *X0 = reinterpret_cast<float2 *>(smem_raw);   // own tile   [N][LT]
+    float2 *X1 = X0 + N * LT;                           // mirror tile [N][LT]
+    constexpr int NT = 16 * LT;
+    const int lane = threadIdx.x % LT;
     const int ky = blockIdx.x / TILES;
-    const int kz = (blockIdx.x % TILES) * kLT + lane;
+    const int kz = (blockIdx.x % TILES) * LT + lane;
     const bool ok = kz < N;
     const int kzm = (N - kz) % N;
     const int b = blockIdx.y;
@@ -571,9 +574,9 @@ __global__ void __launch_bounds__(kNT)
         const int kyo = pass == 0 ? ky : NH;   // own row
         const int kym = (N - kyo) % N;         // mirror row
         // forward x pass 1 on both tiles, straight from global (pruned rows)
-        for (int it = threadIdx.x; it < 2 * kLT * R2; it += blockDim.x) {
-            const int s = it / (kLT * R2);
-            const int t = (it / kLT) % R2;
+        for (int it = threadIdx.x; it < 2 * LT * R2; it += blockDim.x) {
+            const int s = it / (LT * R2);
+            const int t = (it / LT) % R2;
             const int row = s ? kym : kyo, col = s ? kzm : kz;
             float2 v[R1];
             static_for<0, R1>([&](auto m_) {
@@ -591,21 +594,21 @@ __global__ void __launch_bounds__(kNT)
                 constexpr int k1 = decltype(k1_)::value;
                 float2 x = v[k1];
                 if constexpr (k1 != 0) x = cmul(x, __ldg(&G.tw[t * k1]));
-                X[(k1 * R2 + t) * kLT + lane] = x;
+                X[(k1 * R2 + t) * LT + lane] = x;
             });
         }
         __syncthreads();
         // forward x pass 2 and the conj(R^) product, held in registers
-        constexpr int IPT = (2 * kLT * R1 + kNT - 1) / kNT;
+        constexpr int IPT = (2 * LT * R1 + NT - 1) / NT;
         float2 reg[IPT][R2];
 #pragma unroll
         for (int r = 0; r < IPT; ++r) {
-            const int it = threadIdx.x + r * kNT;
-            if (it < 2 * kLT * R1) {
-                const int s = it / (kLT * R1);
-                const int u = (it / kLT) % R1;
+            const int it = threadIdx.x + r * NT;
+            if (it < 2 * LT * R1) {
+                const int s = it / (LT * R1);
+                const int u = (it / LT) % R1;
                 const int row = s ? kym : kyo, col = s ? kzm : kz;
-                fft_phase2<N, -1>((s ? X1 : X0) + lane, kLT, u, reg[r]);
+                fft_phase2<N, -1>((s ? X1 : X0) + lane, LT, u, reg[r]);
                 static_for<0, R2>([&](auto k2) {
                     const int kx = u + R1 * k2;
                     const float2 rh = ok ? __ldg(&Rh[((size_t)kx * N + row) * N + col]) : make_float2(0.f, 0.f);
@@ -616,24 +619,24 @@ __global__ void __launch_bounds__(kNT)
         __syncthreads();
 #pragma unroll
         for (int r = 0; r < IPT; ++r) {
-            const int it = threadIdx.x + r * kNT;
-            if (it < 2 * kLT * R1) {
-                const int s = it / (kLT * R1);
-                const int u = (it / kLT) % R1;
+            const int it = threadIdx.x + r * NT;
+            if (it < 2 * LT * R1) {
+                const int s = it / (LT * R1);
+                const int u = (it / LT) % R1;
                 float2 *X = s ? X1 : X0;
-                static_for<0, R2>([&](auto k2) { X[(u + R1 * k2) * kLT + lane] = reg[r][k2]; });
+                static_for<0, R2>([&](auto k2) { X[(u + R1 * k2) * LT + lane] = reg[r][k2]; });
             }
         }
         __syncthreads();
         // inverse x pass 1 of H = (P_own(kx) + conj(P_mirror(-kx))) / 2, in place in X0
-        for (int it = threadIdx.x; it < kLT * R2; it += blockDim.x) {
-            const int t = it / kLT;
+        for (int it = threadIdx.x; it < LT * R2; it += blockDim.x) {
+            const int t = it / LT;
             float2 v[R1];
             static_for<0, R1>([&](auto m_) {
                 constexpr int mm = decltype(m_)::value;
                 const int e = t + R2 * mm;
-                const float2 a = X0[e * kLT + lane];
-                const float2 c = X1[((N - e) % N) * kLT + lane];
+                const float2 a = X0[e * LT + lane];
+                const float2 c = X1[((N - e) % N) * LT + lane];
                 v[mm] = make_float2(0.5f * (a.x + c.x), 0.5f * (a.y - c.y));
             });
             Dft<R1, +1>::run(v);
@@ -641,15 +644,15 @@ __global__ void __launch_bounds__(kNT)
                 constexpr int k1 = decltype(k1_)::value;
                 float2 x = v[k1];
                 if constexpr (k1 != 0) x = cmul(x, conjf2(__ldg(&G.tw[t * k1])));
-                X0[(k1 * R2 + t) * kLT + lane] = x;
+                X0[(k1 * R2 + t) * LT + lane] = x;
             });
         }
         __syncthreads();
         // inverse x pass 2 -> Gh (row 0 packs ky = 0 and ky = N/2)
-        for (int it = threadIdx.x; it < kLT * R1; it += blockDim.x) {
-            const int u = it / kLT;
+        for (int it = threadIdx.x; it < LT * R1; it += blockDim.x) {
+            const int u = it / LT;
             float2 o[R2];
-            fft_phase2<N, +1>(X0 + lane, kLT, u, o);
+            fft_phase2<N, +1>(X0 + lane, LT, u, o);
             if (ok) {
                 static_for<0, R2>([&](auto k2) {
                     const int x = u + R1 * k2;

@@ -105,6 +105,7 @@ struct md_ctx {
     // work sets (lane 0 serves every form; lane 1 the batched graph)
     int batch = 1;
     int plan = 0;   // radix plan variant of the plane top-t kernel (C2RPlan)
+    int tile = 32;  // kz lines per CTA of the x-line kernel (16 or 32)
     int cap = 0, cap_t = 0, cap_na = 0;
     WorkSet::Sizes have{};           // bytes held by each work-set buffer
     WorkSet ws[kLanes];
@@ -139,7 +140,8 @@ struct Sized {
     static constexpr int NH = N / 2;
     static constexpr int TILES = (N + kLT - 1) / kLT;
     static size_t smem_fwd() { return (size_t)N * (N + 1) * sizeof(float2); }
-    static size_t smem_xline() { return (size_t)2 * N * kLT * sizeof(float2); }
+    template <int LT = kLT>
+    static size_t smem_xline() { return (size_t)2 * N * LT * sizeof(float2); }
     template <int V = 0>
     static size_t smem_c2r() {
         constexpr int PA = N + C2RPlan<N, V>::R1, PB = N + 8;
@@ -156,7 +158,8 @@ struct Sized {
         set((const void *)k_plane_fwd<N, 0>, smem_fwd());
         set((const void *)k_plane_fwd<N, 1>, smem_fwd());
         set((const void *)k_plane_fwd<N, 2>, smem_fwd());
-        set((const void *)k_xline_herm<N>, smem_xline());
+        set((const void *)k_xline_herm<N, 32>, smem_xline<32>());
+        set((const void *)k_xline_herm<N, 16>, smem_xline<16>());
         set((const void *)k_plane_c2r<N, 1, 0>, smem_c2r<0>());
         set((const void *)k_plane_c2r<N, 4, 0>, smem_c2r<0>());
         set((const void *)k_plane_c2r<N, 16, 0>, smem_c2r<0>());
@@ -243,7 +246,10 @@ struct Sized {
         k_plane_fwd<N, 0><<<dim3(NG, nb), kNT1, smem_fwd(), s>>>(L, G, w.vbits, w.qlist, w.qcount, nullptr, nullptr,
                                                                 w.A, nullptr, nullptr);
         if (ev) cudaEventRecord(ev[2], s);
-        k_xline_herm<N><<<dim3(NH * TILES, nb), kNT, smem_xline(), s>>>(G, w.A, c->d_Rh, w.G);
+        if (c->tile == 16)
+            k_xline_herm<N, 16><<<dim3(NH * ((N + 15) / 16), nb), 256, smem_xline<16>(), s>>>(G, w.A, c->d_Rh, w.G);
+        else
+            k_xline_herm<N, 32><<<dim3(NH * ((N + 31) / 32), nb), 512, smem_xline<32>(), s>>>(G, w.A, c->d_Rh, w.G);
         if (ev) cudaEventRecord(ev[3], s);
         plane_topt(s, G, w.G, nb, t, nf3f, w.cand, c->plan);
         if (ev) cudaEventRecord(ev[4], s);
@@ -742,6 +748,15 @@ int md_ligand_data(md_ctx *ctx, int na, const float *xyz, const float *radius, c
 int md_set_batch(md_ctx *ctx, int b) {
     if (!ctx || b < 1) return MD_ERR_ARG;
     ctx->batch = b;
+    return MD_OK;
+}
+
+int md_set_tile(md_ctx *ctx, int lines) {
+    if (!ctx || (lines != 16 && lines != 32)) return MD_ERR_ARG;
+    if (lines != ctx->tile) {
+        free_graphs(ctx);
+        ctx->tile = lines;
+    }
     return MD_OK;
 }
 

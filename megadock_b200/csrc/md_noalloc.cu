@@ -82,7 +82,7 @@ cudaError_t set_attrs() {
         if (e == cudaSuccess) e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
     };
     set((const void *)k_plane_fwd<N, 0>, Smem<N>::fwd());
-    set((const void *)k_xline_herm<N>, Smem<N>::xline());
+    set((const void *)k_xline_herm<N, kLT>, Smem<N>::xline());
     set((const void *)k_plane_c2r<N, 1>, Smem<N>::c2r());
     set((const void *)k_plane_c2r<N, 4>, Smem<N>::c2r());
     set((const void *)k_plane_c2r<N, 16>, Smem<N>::c2r());
@@ -144,7 +144,7 @@ void run_rotation(cudaStream_t s, const LigandView &L, const GridView &G, const 
     k_vox_bits<NG><<<dim3(NG, 1), kNT0, 0, s>>>(L, G, pr.srec, pr.sstart, pr.cq, pr.cstart, vbits, qlist, qcount);
     k_plane_fwd<N, 0><<<dim3(NG, 1), kNT1, Smem<N>::fwd(), s>>>(L, G, vbits, qlist, qcount, nullptr, nullptr, A,
                                                                nullptr, nullptr);
-    k_xline_herm<N><<<dim3(NH * TILES, 1), kNT, Smem<N>::xline(), s>>>(G, A, Rh, Gsp);
+    k_xline_herm<N, kLT><<<dim3(NH * TILES, 1), 16 * kLT, Smem<N>::xline(), s>>>(G, A, Rh, Gsp);
     const int T = t == 1 ? 1 : (t <= 4 ? 4 : 16);
     for (int out0 = 0; out0 < t; out0 += T) {
         const int nsel = t - out0 < T ? t - out0 : T;

@@ -34,6 +34,7 @@ class FFTProcess:
         self._h = h
         self.num_fft = 0
         self._top = None
+        self.plan, self.tile = 0, 32
         if stream is not None:
             _check(N.lib().md_set_stream(self._h, C.c_void_p(stream)), self._h)
 
@@ -85,6 +86,11 @@ class FFTProcess:
 
     def set_batch(self, rotations_per_launch: int):
         _check(N.lib().md_set_batch(self._h, int(rotations_per_launch)), self._h)
+
+    def set_tile(self, lines: int):
+        """kz lines per CTA of the x-line kernel (16 or 32)."""
+        _check(N.lib().md_set_tile(self._h, int(lines)), self._h)
+        self.tile = int(lines)
 
     def set_plan(self, plan: int):
         """Radix plan variant of the inverse plane kernel (0, 1 or 2)."""

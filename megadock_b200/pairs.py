@@ -96,16 +96,18 @@ class PairBatch:
         self.d_rot = torch.from_numpy(mats).to(f"cuda:{device}")
         self.d_out = [torch.zeros(self.n_rot * t * 5, dtype=torch.int32, device=f"cuda:{device}")
                       for _ in self.ctxs]
-        self.batch_by_n, self.plan_by_n = {}, {}
+        self.batch_by_n, self.plan_by_n, self.tile_by_n = {}, {}, {}
         if autotune:
             from .tune import autotune
             for fp in self.ctxs:
                 if fp.num_fft not in self.batch_by_n:
                     self.batch_by_n[fp.num_fft], self.plan_by_n[fp.num_fft] = autotune(
                         fp, self.d_rot.data_ptr(), self.d_out[0].data_ptr(), t, sample=min(768, self.n_rot))
+                    self.tile_by_n[fp.num_fft] = fp.tile
         for fp in self.ctxs:
             fp.set_batch(self.batch_by_n.get(fp.num_fft, 16))
             fp.set_plan(self.plan_by_n.get(fp.num_fft, 0))
+            fp.set_tile(self.tile_by_n.get(fp.num_fft, 32))
         self.runner = FFTProcess(device, stream=stream)
 
     def run(self, stream=None):

@@ -1,14 +1,16 @@
-"""Autotuner for the batched form: rotations per launch and radix plan.
+"""Autotuner for the batched form: rotations per launch, radix plan and tile.
 
 The batched pipeline's cost per rotation falls as more rotations share a
 launch (fuller grids, fewer launches) until the per-launch intermediates stop
 fitting in L2, and the inverse plane kernel (the largest stage) runs at
 different speeds with different radix splits of its two axes (md_set_plan:
 variant 0 the line plans, 1 the kz split reversed, 2 the ky split reversed),
-depending on the size.  ``autotune`` times a sample of rotations with the
-library's per-stage CUDA events (md_dock_profile): first every batch size with
-plan 0, then every plan at the best batch, and keeps the fastest pair.
-Results are cached per (N, t, sample) in-process.
+depending on the size, and the x-line kernel works on tiles of 16 or 32 kz
+lines per CTA (md_set_tile).  ``autotune`` times a sample of rotations with
+the library's per-stage CUDA events (md_dock_profile): first every batch size
+with plan 0 and 32-line tiles, then every plan at the best batch, then the
+other tile, and keeps the fastest combination.  Results are cached per
+(N, t, sample) in-process.
 """
 from __future__ import annotations
 
@@ -16,6 +18,7 @@ _cache: dict = {}
 
 CANDIDATES = (4, 8, 16, 24, 32, 48, 64)
 PLANS = (0, 1, 2)
+TILES = (32, 16)
 
 
 def _time(fp, d_rotmat, d_out, t, sample, b):
@@ -26,15 +29,18 @@ def _time(fp, d_rotmat, d_out, t, sample, b):
 
 
 def autotune(fp, d_rotmat: int, d_out: int, t: int, sample: int = 1536, candidates=CANDIDATES,
-             plans=PLANS) -> tuple[int, int]:
-    """(rotations per launch, plan) for context fp, left set on fp."""
-    key = (fp.num_fft, t, sample, tuple(candidates), tuple(plans))
+             plans=PLANS, tiles=TILES) -> tuple[int, int]:
+    """(rotations per launch, plan) for context fp; batch, plan and tile are
+    left set on fp (the tile is fp.tile)."""
+    key = (fp.num_fft, t, sample, tuple(candidates), tuple(plans), tuple(tiles))
     if key in _cache:
-        b, p = _cache[key]
+        b, p, tl = _cache[key]
         fp.set_batch(b)
         fp.set_plan(p)
+        fp.set_tile(tl)
         return b, p
     fp.set_plan(plans[0])
+    fp.set_tile(tiles[0])
     best_b, best_ms = candidates[0], float("inf")
     for b in candidates:
         ms = _time(fp, d_rotmat, d_out, t, sample, b)
@@ -46,9 +52,16 @@ def autotune(fp, d_rotmat: int, d_out: int, t: int, sample: int = 1536, candidat
         ms = _time(fp, d_rotmat, d_out, t, sample, best_b)
         if ms < best_ms:
             best_p, best_ms = p, ms
-    fp.set_batch(best_b)
     fp.set_plan(best_p)
-    _cache[key] = (best_b, best_p)
+    best_t = tiles[0]
+    for tl in tiles[1:]:
+        fp.set_tile(tl)
+        ms = _time(fp, d_rotmat, d_out, t, sample, best_b)
+        if ms < best_ms:
+            best_t, best_ms = tl, ms
+    fp.set_batch(best_b)
+    fp.set_tile(best_t)
+    _cache[key] = (best_b, best_p, best_t)
     return best_b, best_p
 
 

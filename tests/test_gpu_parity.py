@@ -162,6 +162,19 @@ def test_dock_matches_reference_fp32(built, gpu, pairs):
     print(f"\nvs the reference's FP32 path (project FFT shim): max relative error {max(errs):.2e}")
 
 
+def test_xline_tiles_bit_identical(built, gpu, pairs):
+    """16- and 32-line tiles of the x-line kernel compute the same lines."""
+    from megadock_b200 import rotation_matrices
+    for name, extra in (("c0", ("-F", "96", "-r", "360")), ("small", ("-F", "100", "-r", "360"))):
+        job, fp = _setup(pairs, name, *extra)
+        mats = rotation_matrices(job.rotation_angles()[:48])
+        fp.set_batch(16)
+        a = fp.cuda_fft(mats, t=3).copy()
+        fp.set_tile(16)
+        b = fp.cuda_fft(mats, t=3).copy()
+        assert np.array_equal(a, b), name
+
+
 def test_batched_equals_plain(built, gpu, pairs):
     from megadock_b200 import rotation_matrices
     job, fp = _setup(pairs, "c0", "-F", "96", "-r", "360", "-t", "3")
