@@ -80,8 +80,8 @@ int md_set_batch(md_ctx *ctx, int rotations_per_launch);
  * 1 the kz split reversed, 2 the ky split reversed (t <= 4; larger t uses 0).
  * The autotuner (megadock_b200.tune) picks it together with the batch. */
 int md_set_plan(md_ctx *ctx, int plan);
-/* Tile shape of the x-line kernel: 16 or 32 kz lines per CTA (default 32);
- * also picked by the autotuner. */
+/* Tile shape of the x-line kernel: 8, 16 or 32 kz lines per CTA (default
+ * 32); also picked by the autotuner. */
 int md_set_tile(md_ctx *ctx, int lines);
 
 /* FFTProcess::cuda_fft (src/fft_process.cpp:502-656) over rotations

@@ -88,7 +88,7 @@ class FFTProcess:
         _check(N.lib().md_set_batch(self._h, int(rotations_per_launch)), self._h)
 
     def set_tile(self, lines: int):
-        """kz lines per CTA of the x-line kernel (16 or 32)."""
+        """kz lines per CTA of the x-line kernel (8, 16 or 32)."""
         _check(N.lib().md_set_tile(self._h, int(lines)), self._h)
         self.tile = int(lines)
 

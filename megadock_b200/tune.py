@@ -5,11 +5,11 @@ launch (fuller grids, fewer launches) until the per-launch intermediates stop
 fitting in L2, and the inverse plane kernel (the largest stage) runs at
 different speeds with different radix splits of its two axes (md_set_plan:
 variant 0 the line plans, 1 the kz split reversed, 2 the ky split reversed),
-depending on the size, and the x-line kernel works on tiles of 16 or 32 kz
-lines per CTA (md_set_tile).  ``autotune`` times a sample of rotations with
+depending on the size, and the x-line kernel works on tiles of 8, 16 or 32
+kz lines per CTA (md_set_tile).  ``autotune`` times a sample of rotations with
 the library's per-stage CUDA events (md_dock_profile): first every batch size
 with plan 0 and 32-line tiles, then every plan at the best batch, then the
-other tile, and keeps the fastest combination.  Results are cached per
+other tiles, and keeps the fastest combination.  Results are cached per
 (N, t, sample) in-process.
 """
 from __future__ import annotations
@@ -18,7 +18,7 @@ _cache: dict = {}
 
 CANDIDATES = (4, 8, 16, 24, 32, 48, 64)
 PLANS = (0, 1, 2)
-TILES = (32, 16)
+TILES = (32, 16, 8)
 
 
 def _time(fp, d_rotmat, d_out, t, sample, b):

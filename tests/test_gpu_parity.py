@@ -163,16 +163,17 @@ def test_dock_matches_reference_fp32(built, gpu, pairs):
 
 
 def test_xline_tiles_bit_identical(built, gpu, pairs):
-    """16- and 32-line tiles of the x-line kernel compute the same lines."""
+    """8-, 16- and 32-line tiles of the x-line kernel compute the same lines."""
     from megadock_b200 import rotation_matrices
     for name, extra in (("c0", ("-F", "96", "-r", "360")), ("small", ("-F", "100", "-r", "360"))):
         job, fp = _setup(pairs, name, *extra)
         mats = rotation_matrices(job.rotation_angles()[:48])
         fp.set_batch(16)
         a = fp.cuda_fft(mats, t=3).copy()
-        fp.set_tile(16)
-        b = fp.cuda_fft(mats, t=3).copy()
-        assert np.array_equal(a, b), name
+        for tile in (16, 8):
+            fp.set_tile(tile)
+            b = fp.cuda_fft(mats, t=3).copy()
+            assert np.array_equal(a, b), (name, tile)
 
 
 def test_batched_equals_plain(built, gpu, pairs):
