@@ -174,6 +174,8 @@ def run_profile_case(args):
         xyz, rad, q = job.ligand_atoms()
         fp.ligand_data_transfer_gpu(xyz, rad, q, job.lig_core)
         fp.set_batch(args.batch or 16)
+        fp.set_plan(args.plan)
+        fp.set_tile(args.tile)
         d_rot = torch.from_numpy(mats).cuda()
         d_pose = torch.zeros(len(mats) * T_POSES * 5, dtype=torch.int32, device="cuda")
         fp.dock_profile(d_rot.data_ptr(), 0, len(mats), T_POSES, d_pose.data_ptr())
@@ -386,8 +388,10 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--batch", type=int, default=0, help="rotations per launch (0 = autotune batch and plan)")
-    ap.add_argument("--plan", type=int, default=0, help="inverse plane kernel radix plan with --batch (0, 1, 2)")
-    ap.add_argument("--tile", type=int, default=32, help="x-line kernel kz lines per CTA with --batch (16, 32)")
+    ap.add_argument("--plan", type=int, default=0,
+                    help="inverse plane kernel radix plan with --batch or --profile-case (0, 1, 2)")
+    ap.add_argument("--tile", type=int, default=32,
+                    help="x-line kernel kz lines per CTA with --batch or --profile-case (8, 16, 32)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="metric", choices=["metric", "pairs", "adjoint", "fit"],
                     help="metric: the headline workload; pairs: 64 uneven synthetic pairs, 3,600 rotations each; "
