@@ -731,10 +731,15 @@ struct TopList {
             i[j] = -1;
         }
     }
+    // FLOOR: a floor from an earlier pass is in force (uniform per launch).
+    // The common case -- a full list and a key that is not better than its
+    // last entry -- is one predicate of non-short-circuit comparisons.
+    template <bool FLOOR = true>
     __device__ __forceinline__ void insert(float key, int idx, const Cand &floor) {
-        if (!(key == key)) return;   // NaN
-        if (floor.idx >= 0 && !key_better(floor.key, floor.idx, key, idx)) return;
-        if (i[T - 1] >= 0 && !key_better(key, idx, k[T - 1], i[T - 1])) return;
+        const bool full = i[T - 1] >= 0;
+        const bool beats_last = (key > k[T - 1]) | ((key == k[T - 1]) & (idx < i[T - 1]));
+        if ((full & !beats_last) | !(key == key)) return;   // not better than the list, or NaN
+        if (FLOOR && floor.idx >= 0 && !key_better(floor.key, floor.idx, key, idx)) return;
 #pragma unroll
         for (int j = 0; j < T; ++j) {
             if (i[j] < 0 || key_better(key, idx, k[j], i[j])) {
@@ -903,22 +908,27 @@ __global__ void __launch_bounds__(kNT, c2r_min_blocks<N, T, V>())
         }
     }
     const int base = x * N * N;
-    for (int it = tid; it < N * Q1; it += blockDim.x) {
-        const int z = it % N, u = it / N;
-        float2 o[Q2];
-        static_for<0, Q2>([&](auto n2_) {
-            constexpr int n2 = decltype(n2_)::value;
-            o[n2] = S[(u * Q2 + n2) * PITCH + z];
-        });
-        Dft<Q2, +1>::run(o);
-        static_for<0, Q2>([&](auto k2_) {
-            constexpr int k2 = decltype(k2_)::value;
-            const int m2 = u + Q1 * k2;
-            const float se = o[k2].x, so = o[k2].y;
-            top.insert(se, base + (2 * m2) * N + z, floor);
-            top.insert(so, base + (2 * m2 + 1) * N + z, floor);
-        });
-    }
+    auto scan = [&](auto floor_on) {
+        constexpr bool FL = decltype(floor_on)::value;
+        for (int it = tid; it < N * Q1; it += blockDim.x) {
+            const int z = it % N, u = it / N;
+            float2 o[Q2];
+            static_for<0, Q2>([&](auto n2_) {
+                constexpr int n2 = decltype(n2_)::value;
+                o[n2] = S[(u * Q2 + n2) * PITCH + z];
+            });
+            Dft<Q2, +1>::run(o);
+            const int cell0 = base + 2 * u * N + z;
+            static_for<0, Q2>([&](auto k2_) {
+                constexpr int k2 = decltype(k2_)::value;
+                constexpr int step = 2 * Q1 * k2 * N;   // 2 m2 N - 2 u N for m2 = u + Q1 k2
+                top.template insert<FL>(o[k2].x, cell0 + step, floor);
+                top.template insert<FL>(o[k2].y, cell0 + step + N, floor);
+            });
+        }
+    };
+    if (floor.idx >= 0) scan(std::true_type{});
+    else scan(std::false_type{});
     // block merge: nsel rounds over the per-thread heads
     for (int r = 0; r < nsel; ++r) {
         Cand mine{top.k[0], top.i[0]};
