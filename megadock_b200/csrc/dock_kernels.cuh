@@ -23,6 +23,8 @@
 //   FFT / product      src/fft_process.cpp:333-396 (FFTW) and :537-558 (cuFFT)
 //   top-t              src/fft_process.cpp:399-458
 #pragma once
+#include <climits>
+
 #include "fft_dev.cuh"
 
 namespace mdb {
@@ -718,8 +720,12 @@ __device__ __forceinline__ Cand block_best(Cand mine, Cand *red) {
 }
 
 // Per-thread sorted list of the T best (key, index) pairs seen, best first.
-// Only candidates strictly after `floor` in selection order are kept (used
-// when a plane's top-t is found in several passes of T).
+// Empty slots hold (-inf, INT_MAX), which every non-NaN key beats, so the
+// one test against the last slot rejects NaN, too-small keys and equal keys
+// of later cells alike; an accepted key enters through a branch-free
+// compare-and-select network (the list is sorted, so "beats slot j" implies
+// "beats slot j+1").  Only candidates strictly after `floor` in selection
+// order are kept (used when a plane's top-t is found in several passes of T).
 template <int T>
 struct TopList {
     float k[T];
@@ -727,39 +733,36 @@ struct TopList {
     __device__ __forceinline__ void init() {
 #pragma unroll
         for (int j = 0; j < T; ++j) {
-            k[j] = 0.f;
-            i[j] = -1;
+            k[j] = -INFINITY;
+            i[j] = INT_MAX;
         }
     }
     // FLOOR: a floor from an earlier pass is in force (uniform per launch).
-    // The common case -- a full list and a key that is not better than its
-    // last entry -- is one predicate of non-short-circuit comparisons.
     template <bool FLOOR = true>
     __device__ __forceinline__ void insert(float key, int idx, const Cand &floor) {
-        const bool full = i[T - 1] >= 0;
-        const bool beats_last = (key > k[T - 1]) | ((key == k[T - 1]) & (idx < i[T - 1]));
-        if ((full & !beats_last) | !(key == key)) return;   // not better than the list, or NaN
+        if (!((key > k[T - 1]) | ((key == k[T - 1]) & (idx < i[T - 1])))) return;
         if (FLOOR && floor.idx >= 0 && !key_better(floor.key, floor.idx, key, idx)) return;
+        bool b[T];
 #pragma unroll
-        for (int j = 0; j < T; ++j) {
-            if (i[j] < 0 || key_better(key, idx, k[j], i[j])) {
-                const float tk = k[j];
-                const int ti = i[j];
-                k[j] = key;
-                i[j] = idx;
-                key = tk;
-                idx = ti;
-                if (idx < 0) break;
-            }
+        for (int j = 0; j < T; ++j) b[j] = (key > k[j]) | ((key == k[j]) & (idx < i[j]));
+#pragma unroll
+        for (int j = T - 1; j >= 1; --j) {
+            k[j] = b[j - 1] ? k[j - 1] : (b[j] ? key : k[j]);
+            i[j] = b[j - 1] ? i[j - 1] : (b[j] ? idx : i[j]);
         }
+        k[0] = b[0] ? key : k[0];
+        i[0] = b[0] ? idx : i[0];
     }
+    // the best entry as a candidate (index -1 when the list is empty)
+    __device__ __forceinline__ Cand head() const { return Cand{k[0], i[0] == INT_MAX ? -1 : i[0]}; }
     __device__ __forceinline__ void pop() {
 #pragma unroll
         for (int j = 0; j < T - 1; ++j) {
             k[j] = k[j + 1];
             i[j] = i[j + 1];
         }
-        i[T - 1] = -1;
+        k[T - 1] = -INFINITY;
+        i[T - 1] = INT_MAX;
     }
 };
 
@@ -931,7 +934,7 @@ __global__ void __launch_bounds__(kNT, c2r_min_blocks<N, T, V>())
     else scan(std::false_type{});
     // block merge: nsel rounds over the per-thread heads
     for (int r = 0; r < nsel; ++r) {
-        Cand mine{top.k[0], top.i[0]};
+        Cand mine = top.head();
         const Cand best = block_best(mine, red);
         if (tid == 0) out[r] = best;
         if (best.idx < 0) {
