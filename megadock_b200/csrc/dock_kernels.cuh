@@ -807,7 +807,6 @@ __global__ void __launch_bounds__(kNT, c2r_min_blocks<N, T, V>())
     constexpr int PITCH = PA > PB ? PA : PB;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     float2 *S = reinterpret_cast<float2 *>(smem_raw);   // NH x PITCH
-    __shared__ Cand red[33];
     const int x = blockIdx.x;
     const int b = blockIdx.y;
     const int tid = threadIdx.x;
@@ -932,17 +931,50 @@ __global__ void __launch_bounds__(kNT, c2r_min_blocks<N, T, V>())
     };
     if (floor.idx >= 0) scan(std::true_type{});
     else scan(std::false_type{});
-    // block merge: nsel rounds over the per-thread heads
-    for (int r = 0; r < nsel; ++r) {
-        Cand mine = top.head();
-        const Cand best = block_best(mine, red);
-        if (tid == 0) out[r] = best;
-        if (best.idx < 0) {
-            if (tid == 0)
-                for (int r2 = r + 1; r2 < nsel; ++r2) out[r2] = Cand{0.f, -1};
-            break;
+    // merge: each warp takes its best nsel from its lanes' lists (shuffles
+    // only), then warp 0 takes the plane's best nsel from the warps' lists,
+    // with one block barrier in between
+    __shared__ Cand wl[kNT / 32][16];
+    const int lane = tid & 31, warp = tid >> 5;
+    auto warp_best = [&](Cand c, int &owner) {
+        owner = lane;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const float k2 = __shfl_down_sync(0xffffffffu, c.key, o);
+            const int i2 = __shfl_down_sync(0xffffffffu, c.idx, o);
+            const int w2 = __shfl_down_sync(0xffffffffu, owner, o);
+            if (i2 >= 0 && (c.idx < 0 || key_better(k2, i2, c.key, c.idx))) {
+                c.key = k2;
+                c.idx = i2;
+                owner = w2;
+            }
         }
-        if (top.i[0] == best.idx) top.pop();
+        c.key = __shfl_sync(0xffffffffu, c.key, 0);
+        c.idx = __shfl_sync(0xffffffffu, c.idx, 0);
+        owner = __shfl_sync(0xffffffffu, owner, 0);
+        return c;
+    };
+    for (int r = 0; r < nsel; ++r) {
+        int owner;
+        const Cand c = warp_best(top.head(), owner);
+        if (lane == 0) wl[warp][r] = c;
+        if (c.idx >= 0 && lane == owner) top.pop();
+    }
+    __syncthreads();
+    if (warp == 0) {
+        const int nw = blockDim.x >> 5;
+        int pos = 0;   // this lane's read position in its warp list
+        for (int r = 0; r < nsel; ++r) {
+            int owner;
+            const Cand c = warp_best((lane < nw && pos < nsel) ? wl[lane][pos] : Cand{0.f, -1}, owner);
+            if (lane == 0) out[r] = c.idx >= 0 ? c : Cand{0.f, -1};
+            if (c.idx < 0) {
+                if (lane == 0)
+                    for (int r2 = r + 1; r2 < nsel; ++r2) out[r2] = Cand{0.f, -1};
+                break;
+            }
+            if (lane == owner) ++pos;
+        }
     }
 }
 
