@@ -297,9 +297,13 @@ def run_adjoint_workload(args):
     fp.alloc_array(job.nf1, job.grid_width, job.grid_coord())
     fp.receptor_fft(rr, ri)
     fp.ligand_data_transfer_gpu(xyz, rad, q, job.lig_core)
-    fp.set_batch(args.batch or 64)
     d_rot = torch.from_numpy(mats).cuda()
     d_pose = torch.zeros(n * 5, dtype=torch.int32, device="cuda")
+    if args.batch:
+        fp.set_batch(args.batch)
+    else:
+        from megadock_b200.tune import autotune
+        autotune(fp, d_rot.data_ptr(), d_pose.data_ptr(), 1)
     state = {}
 
     def fwd():
