@@ -356,7 +356,8 @@ def run_fit_workload(args):
     pairs = []
     for nr, nl, seed in synth.fitting_pairs(args.fit_pairs):
         pc = synth.plant_complex(tmp, nr, nl, seed, rotation_set=54000)
-        pairs.append(FitPair(pc, choose_fft_size(pc.rec_pdb, pc.lig_pdb), 54000, batch=args.batch or 64))
+        pairs.append(FitPair(pc, choose_fft_size(pc.rec_pdb, pc.lig_pdb), 54000, batch=args.batch or None,
+                             tune=not args.batch))
     t_setup = time.perf_counter() - t_setup
     f = Fitter(pairs, alpha=1.0, temperature=10.0)
     state = {}

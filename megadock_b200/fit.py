@@ -71,7 +71,7 @@ class FitPair:
     """One planted complex on the device: its docking context, the receptor's
     per-residue-type field grids and the native pose."""
 
-    def __init__(self, planted, nfft, rotation_set, device=0, batch=None):
+    def __init__(self, planted, nfft, rotation_set, device=0, batch=None, tune=False):
         self.pc = planted
         self.job = Job(["-R", planted.rec_pdb, "-L", planted.lig_pdb, "-F", str(nfft), "-r", str(rotation_set)])
         job = self.job
@@ -95,6 +95,15 @@ class FitPair:
         self.batch = batch
         if batch:
             self.fp.set_batch(batch)
+        if tune:
+            # launch shape of this FFT size (cached per size by the autotuner)
+            import torch
+
+            from .tune import autotune
+            self.set_params(1.0, np.ones(self.K))
+            d_rot = torch.from_numpy(self.mats).to(f"cuda:{device}")
+            d_out = torch.zeros(len(self.mats) * 5, dtype=torch.int32, device=f"cuda:{device}")
+            self.batch, _ = autotune(self.fp, d_rot.data_ptr(), d_out.data_ptr(), 1, sample=min(768, len(self.mats)))
 
     def set_params(self, alpha, scale):
         scale = np.asarray(scale, np.float64)
