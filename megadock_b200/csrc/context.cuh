@@ -151,6 +151,7 @@ struct Sized {
         set((const void *)k_plane_fwd<N, 0>, smem_fwd());
         set((const void *)k_plane_fwd<N, 1>, smem_fwd());
         set((const void *)k_plane_fwd<N, 2>, smem_fwd());
+        if constexpr (fwd_cb_fits<N>()) set((const void *)k_plane_fwd_cb<N>, fwd_cb_smem<N>());
         set((const void *)k_xline_herm<N, 32>, smem_xline<32>());
         set((const void *)k_xline_herm<N, 16>, smem_xline<16>());
         set((const void *)k_xline_herm<N, 8>, smem_xline<8>());
@@ -237,8 +238,11 @@ struct Sized {
         const float nf3f = (float)((long long)N * N * N);
         voxelize(c, w, d_rot9, nb, s);
         if (ev) cudaEventRecord(ev[1], s);
-        k_plane_fwd<N, 0><<<dim3(NG, nb), kNT1, smem_fwd(), s>>>(L, G, w.vbits, w.qlist, w.qcount, nullptr, nullptr,
-                                                                w.A, nullptr, nullptr);
+        if constexpr (fwd_cb_fits<N>())
+            k_plane_fwd_cb<N><<<dim3(NG, nb), kNT1B, fwd_cb_smem<N>(), s>>>(L, G, w.vbits, w.qlist, w.qcount, w.A);
+        else
+            k_plane_fwd<N, 0><<<dim3(NG, nb), kNT1, smem_fwd(), s>>>(L, G, w.vbits, w.qlist, w.qcount, nullptr,
+                                                                    nullptr, w.A, nullptr, nullptr);
         if (ev) cudaEventRecord(ev[2], s);
         if (c->tile == 16)
             k_xline_herm<N, 16><<<dim3(NH * ((N + 15) / 16), nb), 256, smem_xline<16>(), s>>>(G, w.A, c->d_Rh, w.G);

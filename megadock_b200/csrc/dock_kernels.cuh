@@ -506,6 +506,121 @@ __global__ void __launch_bounds__(kNT1, 1)
     }
 }
 
+// K1, column-block form (MODE 0): the same forward plane transform with about
+// half the shared memory, so two CTAs share an SM (used by the batched
+// pipeline wherever two fit: N <= 128; B200 measurement at 12,800 rotations
+// and 64 per launch: 6-10 % more rotations/s at N = 64..112, 0.6 % at 128,
+// identical poses).  The z-FFT results of the
+// NG non-zero rows stay resident (NG x (N+1)); the y-FFT then runs over
+// blocks of CB columns through an N x (CB+1) buffer: pruned phase 1 from the
+// resident rows into the block buffer, phase 2 from the block buffer
+// straight to global memory.
+constexpr int kNT1B = 512;
+
+template <int N>
+constexpr size_t fwd_cb_smem() {
+    constexpr int CB = 32;
+    return ((size_t)(N / 2) * (N + 1) + (size_t)N * (CB + 1)) * sizeof(float2);
+}
+
+// two CTAs and their 1 KB system reservations within the SM's 228 KB
+template <int N>
+constexpr bool fwd_cb_fits() {
+    return fwd_cb_smem<N>() <= 113 * 1024;
+}
+
+template <int N>
+__global__ void __launch_bounds__(kNT1B, 2)
+    k_plane_fwd_cb(LigandView L, GridView G, const uint32_t *__restrict__ vbits, const int2 *__restrict__ qlist,
+                   const int *__restrict__ qcount, float2 *__restrict__ A) {
+    constexpr int NG = N / 2, OFF = N / 4, PZ = N + 1, CB = 32, PB = CB + 1;
+    constexpr int R1 = Plan<N>::R1, R2 = Plan<N>::R2;
+    constexpr int W = VoxShared<NG>::W;
+    static_assert(R1 % 4 == 0, "pruned y pass needs R1 % 4 == 0");
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    float2 *Z = reinterpret_cast<float2 *>(smem_raw);   // NG rows x PZ
+    float2 *Y = Z + NG * PZ;                             // N rows x PB
+    const int p = blockIdx.x, b = blockIdx.y, tid = threadIdx.x;
+
+    // the plane's NG rows at column offset OFF (the pruned passes read no
+    // other column)
+    const uint32_t *vb = vbits + ((size_t)b * NG + p) * 2 * NG * W;
+    for (int c = tid; c < NG * NG; c += blockDim.x) {
+        const int q = c / NG, s = c % NG;
+        const uint32_t bit = 1u << (s & 31);
+        const float v = (__ldg(&vb[q * W + (s >> 5)]) & bit) ? L.delta
+                        : (__ldg(&vb[NG * W + q * W + (s >> 5)]) & bit) ? 1.0f : 0.0f;
+        Z[q * PZ + s + OFF] = make_float2(v, 0.f);
+    }
+    __syncthreads();
+    const int nq = qcount[(size_t)b * NG + p];
+    const int2 *ql = qlist + ((size_t)b * NG + p) * NG * NG;
+    for (int e = tid; e < nq; e += blockDim.x) {
+        const int2 c = ql[e];
+        Z[(c.x / NG) * PZ + c.x % NG + OFF].y = __int_as_float(c.y);
+    }
+    __syncthreads();
+    // z-FFT of the NG rows (lanes = rows, pruned columns)
+    for (int it = tid; it < NG * R2; it += blockDim.x) {
+        const int t = it / NG, q = it % NG;
+        fft_phase1<N, -1, true>(Z + q * PZ, 1, t, G.tw);
+    }
+    __syncthreads();
+    {
+        constexpr int IPT = (NG * R1 + kNT1B - 1) / kNT1B;
+        float2 reg[IPT][R2];
+#pragma unroll
+        for (int r = 0; r < IPT; ++r) {
+            const int it = tid + r * kNT1B;
+            if (it < NG * R1) fft_phase2<N, -1>(Z + (it % NG) * PZ, 1, it / NG, reg[r]);
+        }
+        __syncthreads();
+#pragma unroll
+        for (int r = 0; r < IPT; ++r) {
+            const int it = tid + r * kNT1B;
+            if (it < NG * R1) {
+                float2 *row = Z + (it % NG) * PZ;
+                const int u = it / NG;
+                static_for<0, R2>([&](auto k2) { row[u + R1 * k2] = reg[r][k2]; });
+            }
+        }
+    }
+    __syncthreads();
+    // y-FFT of the N columns, CB at a time
+    float2 *Ab = A + ((size_t)b * NG + p) * N * N;
+    for (int cb = 0; cb < N; cb += CB) {
+        for (int it = tid; it < CB * R2; it += blockDim.x) {
+            const int t = it / CB, c = it % CB;
+            if (cb + c >= N) continue;
+            float2 v[R1];
+            static_for<0, R1>([&](auto m_) {
+                constexpr int m = decltype(m_)::value;
+                if constexpr (m < R1 / 4 || m >= 3 * R1 / 4) {
+                    v[m] = make_float2(0.f, 0.f);
+                } else {
+                    v[m] = Z[(t + R2 * (m - R1 / 4)) * PZ + cb + c];   // row n - OFF, n = t + R2 m
+                }
+            });
+            Dft<R1, -1>::run(v);
+            static_for<0, R1>([&](auto k1_) {
+                constexpr int k1 = decltype(k1_)::value;
+                float2 x = v[k1];
+                if constexpr (k1 != 0) x = cmul(x, __ldg(&G.tw[t * k1]));
+                Y[(k1 * R2 + t) * PB + c] = x;
+            });
+        }
+        __syncthreads();
+        for (int it = tid; it < CB * R1; it += blockDim.x) {
+            const int u = it / CB, c = it % CB;
+            if (cb + c >= N) continue;
+            float2 o[R2];
+            fft_phase2<N, -1>(Y + c, PB, u, o);
+            static_for<0, R2>([&](auto k2) { Ab[(size_t)(u + R1 * k2) * N + cb + c] = o[k2]; });
+        }
+        __syncthreads();
+    }
+}
+
 // ------------------------------------------------------------------ K2 (receptor)
 // Forward x-FFT of the ng non-zero spectrum planes of the receptor: writes the
 // full receptor spectrum R^[kx][ky][kz].  CTA = (ky, 32 kz lines); the last
