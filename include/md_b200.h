@@ -76,6 +76,10 @@ int md_ligand_data(md_ctx *ctx, int na, const float *xyz_centred, const float *r
 /* Rotations per launch for md_dock (1 = the plain per-rotation pipeline;
  * > 1 = the batched form, launched as one captured CUDA graph). */
 int md_set_batch(md_ctx *ctx, int rotations_per_launch);
+/* Free the context's rotation work buffers and captured graphs (receptor,
+ * ligand and settings stay); the next docking call allocates them again for
+ * its launch shape.  The autotuner calls it after trying large launch groups. */
+int md_release_work(md_ctx *ctx);
 /* Radix plan of the plane top-t (inverse plane) kernel: 0 the line plans,
  * 1 the kz split reversed, 2 the ky split reversed (t <= 4; larger t uses 0).
  * The autotuner (megadock_b200.tune) picks it together with the batch. */

@@ -469,6 +469,15 @@ int md_set_batch(md_ctx *ctx, int b) {
     return MD_OK;
 }
 
+int md_release_work(md_ctx *ctx) {
+    if (!ctx) return MD_ERR_ARG;
+    MD_CUDA(cudaSetDevice(ctx->device));
+    MD_CUDA(cudaStreamSynchronize(ctx->stream));
+    MD_CUDA(cudaStreamSynchronize(ctx->side));
+    release_work(ctx);
+    return MD_OK;
+}
+
 int md_set_tile(md_ctx *ctx, int lines) {
     if (!ctx || (lines != 8 && lines != 16 && lines != 32)) return MD_ERR_ARG;
     if (lines != ctx->tile) {

@@ -87,6 +87,10 @@ class FFTProcess:
     def set_batch(self, rotations_per_launch: int):
         _check(N.lib().md_set_batch(self._h, int(rotations_per_launch)), self._h)
 
+    def release_work(self):
+        """Free the rotation work buffers (allocated again by the next call)."""
+        _check(N.lib().md_release_work(self._h), self._h)
+
     def set_tile(self, lines: int):
         """kz lines per CTA of the x-line kernel (8, 16 or 32)."""
         _check(N.lib().md_set_tile(self._h, int(lines)), self._h)

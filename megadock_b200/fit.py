@@ -146,6 +146,9 @@ class FitPair:
         keep = np.flatnonzero(wf != 0)
         poses = np.concatenate([self.pos, neg])[keep]
         g = self.fp.adjoint_poses(self.mats[poses["rot"]], poses, wf[keep])
+        # the rotation work buffers (GBs at large launch groups) are freed
+        # between evaluations so that every pair's context fits on the device
+        self.fp.release_work()
         dri = g["d_rec_i"].reshape(-1).astype(np.float64)
         scale = np.asarray(scale, np.float64)
         d_alpha = float(dri @ (scale @ self.U))

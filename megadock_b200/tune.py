@@ -9,16 +9,27 @@ depending on the size, and the x-line kernel works on tiles of 8, 16 or 32
 kz lines per CTA (md_set_tile).  ``autotune`` times a sample of rotations with
 the library's per-stage CUDA events (md_dock_profile): first every batch size
 with plan 0 and 32-line tiles, then every plan at the best batch, then the
-other tiles, and keeps the fastest combination.  Results are cached per
-(N, t, sample) in-process.
+other tiles, and keeps the fastest combination.  Batch sizes whose two work
+sets would exceed WORK_BUDGET bytes are skipped, and the work buffers are
+released at the end so that the next call allocates them for the chosen
+batch only.  Results are cached per (N, t, sample) in-process.
 """
 from __future__ import annotations
 
 _cache: dict = {}
 
-CANDIDATES = (4, 8, 16, 24, 32, 48, 64)
+CANDIDATES = (4, 8, 16, 24, 32, 48, 64, 96, 128, 192)
 PLANS = (0, 1, 2)
 TILES = (32, 16, 8)
+WORK_BUDGET = 12 << 30
+
+
+def work_bytes_per_rotation(n: int) -> int:
+    """Device bytes one rotation of a launch group holds in the two work sets
+    (spectrum planes, Hermitian half, charge lists; the small buffers
+    ignored)."""
+    ng = n // 2
+    return 2 * (8 * ng * n * n + 8 * n * ng * n + 8 * ng ** 3)
 
 
 def _time(fp, d_rotmat, d_out, t, sample, b):
@@ -41,8 +52,9 @@ def autotune(fp, d_rotmat: int, d_out: int, t: int, sample: int = 1536, candidat
         return b, p
     fp.set_plan(plans[0])
     fp.set_tile(tiles[0])
-    best_b, best_ms = candidates[0], float("inf")
-    for b in candidates:
+    fits = [b for b in candidates if b * work_bytes_per_rotation(fp.num_fft) <= WORK_BUDGET] or [candidates[0]]
+    best_b, best_ms = fits[0], float("inf")
+    for b in fits:
         ms = _time(fp, d_rotmat, d_out, t, sample, b)
         if ms < best_ms:
             best_b, best_ms = b, ms
@@ -61,6 +73,7 @@ def autotune(fp, d_rotmat: int, d_out: int, t: int, sample: int = 1536, candidat
             best_t, best_ms = tl, ms
     fp.set_batch(best_b)
     fp.set_tile(best_t)
+    fp.release_work()
     _cache[key] = (best_b, best_p, best_t)
     return best_b, best_p
 

@@ -48,6 +48,7 @@ def test_null_arguments_are_rejected(built):
     assert L.md_adjoint_lse(None, f, 1, None, 10.0, 1.0, None, f, f, f, None, None, 0, f, f) == E
     assert L.md_adjoint_poses(None, f, 1, None, f, f, f, f, None, 0, f, f) == E
     assert L.md_pose_scores(None, f, 1, None, f) == E
+    assert L.md_release_work(None) == E
     assert L.md_pose_terms(None, f, f, 1, None, f) == E
     assert L.md_receptor_build(None, 1, f, f, f, f, -45.0, 1.0, 1.0, 1, f, f) == E
     assert L.md_job_receptor_to(None, None) == E

@@ -20,6 +20,9 @@ class FakeContext:
     def set_tile(self, t):
         self.tile = t
 
+    def release_work(self):
+        self.released = True
+
     def dock_profile(self, d_rot, first, n, t, d_out):
         import numpy as np
         self.calls += 1
@@ -42,3 +45,13 @@ def test_autotune_picks_the_fastest_shape_and_caches():
     fp3 = FakeContext(128, best=(64, 0, 8))
     assert tune.autotune(fp3, 0, 0, 3, sample=256) == (64, 0) and fp3.tile == 8
     assert n == 2 * len(tune.CANDIDATES) + 2 * (len(tune.PLANS) - 1) + 2 * (len(tune.TILES) - 1)
+
+
+def test_autotune_skips_batches_over_the_work_budget():
+    from megadock_b200 import tune
+    tune._cache.clear()
+    fp = FakeContext(160, best=(192, 0, 32))
+    per_rot = tune.work_bytes_per_rotation(160)
+    assert 128 * per_rot <= tune.WORK_BUDGET < 192 * per_rot
+    b, _ = tune.autotune(fp, 0, 0, 3, sample=256)
+    assert b == 128 and fp.released
