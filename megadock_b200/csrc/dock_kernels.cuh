@@ -664,10 +664,20 @@ __global__ void __launch_bounds__(kNT)
 // the pruned forward x-FFT, multiplies both by conj(R^), folds the mirror into
 // H and runs the inverse x-FFT of the own tile.  CTAs of row 0 run two passes
 // (ky = 0 and ky = N/2) and pack them.  Output Gh[x][ky][kz], ky < N/2.
-// LT kz lines per CTA (the tile shape the autotuner picks, 16 or 32), 16 LT
-// threads, 2 * 32 / LT CTAs per SM.
+// LT kz lines per CTA (the tile shape the autotuner picks: 8, 16 or 32), 16 LT
+// threads, xline_occ<N>() / LT CTAs per SM (below).
+//
+// xline_occ: threads per SM the kernel is compiled for, in units of 16:
+// 1,280 where that register budget (51 per thread) holds the kernel without
+// spills, else 1,024.  B200, 13,824 rotations at 192 per launch: +2.0 % at
+// N=96; with spills at N=112 and 128 it lost 2 % and 7 %.
+template <int N>
+constexpr int xline_occ() {
+    return (N == 32 || N == 64 || N == 72 || N == 80 || N == 96) ? 80 : 64;
+}
+
 template <int N, int LT = kLT>
-__global__ void __launch_bounds__(16 * LT, 64 / LT)
+__global__ void __launch_bounds__(16 * LT, xline_occ<N>() / LT)
     k_xline_herm(GridView G, const float2 *__restrict__ A, const float2 *__restrict__ Rh, float2 *__restrict__ Gh) {
     constexpr int NG = N / 2, NH = N / 2, OFF = N / 4;
     constexpr int R1 = Plan<N>::R1, R2 = Plan<N>::R2;
