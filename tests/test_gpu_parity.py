@@ -176,6 +176,23 @@ def test_xline_tiles_bit_identical(built, gpu, pairs):
             assert np.array_equal(a, b), (name, tile)
 
 
+def test_release_work_then_dock_again(built, gpu, pairs):
+    """md_release_work frees the launch groups' buffers and graphs; the next
+    call allocates them again (at another launch shape too) and returns the
+    same records."""
+    from megadock_b200 import rotation_matrices
+    job, fp = _setup(pairs, "c0", "-F", "96", "-r", "360", "-t", "2")
+    mats = rotation_matrices(job.rotation_angles()[:200])
+    fp.set_batch(192)
+    a = fp.cuda_fft(mats, t=2).copy()
+    fp.release_work()
+    b = fp.cuda_fft(mats, t=2).copy()
+    fp.release_work()
+    fp.set_batch(24)
+    c = fp.cuda_fft(mats, t=2).copy()
+    assert np.array_equal(a, b) and np.array_equal(a, c)
+
+
 def test_batched_equals_plain(built, gpu, pairs):
     from megadock_b200 import rotation_matrices
     job, fp = _setup(pairs, "c0", "-F", "96", "-r", "360", "-t", "3")
