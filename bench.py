@@ -106,6 +106,17 @@ def make_inputs(tmp):
     return synth.write_pair(tmp, N_REC, N_LIG, SEED, stem="bench")
 
 
+def workload_config(rp, lp):
+    """The workload's name and sizes, the same for both arms (atoms counted
+    from the generated PDB records)."""
+    def atoms(path):
+        with open(path) as f:
+            return sum(1 for line in f if line.startswith(("ATOM", "HETATM")))
+    return {"workload": f"docking, {N_REC}/{N_LIG}-residue synthetic pair ({atoms(rp)}/{atoms(lp)} atoms), "
+                        f"N={N_FFT}, {ROT_SET} rotations, t={T_POSES}",
+            "fft": N_FFT, "rotations": ROT_SET, "t": T_POSES}
+
+
 def cpu_reference(rp, lp, nrot=REF_SAMPLE_ROT):
     """Time the reference's CPU program (all host cores) on nrot rotations."""
     from oracle import ref
@@ -129,6 +140,7 @@ def run_reference_arm(args):
     from oracle import ref
     with tempfile.TemporaryDirectory() as tmp:
         rp, lp = make_inputs(tmp)
+        config = workload_config(rp, lp)
         if not ref.available():
             print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref (reference compiled from its "
                                                                   "sources) was not built on this machine"}))
@@ -146,9 +158,9 @@ def run_reference_arm(args):
         "impl": "reference", "metric": METRIC, "value": value, "unit": "rotations/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * wall / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": f"plain docking, {N_REC}/{N_LIG}-residue synthetic pair, N={N_FFT}, t={T_POSES}, "
-                               f"sampled {REF_SAMPLE_ROT} of {ROT_SET} rotations per step",
-                   "fft": N_FFT, "rotations": ROT_SET, "t": T_POSES},
+        "config": {**config, "sampled_rotations_per_step": REF_SAMPLE_ROT,
+                   "rate": f"rotations/s of the {REF_SAMPLE_ROT}-rotation sample, the per-rotation cost being "
+                           f"independent of the rotation count"},
         "cpu_baseline": {"value": value, "unit": "rotations/s", "cores": cores, "kind": "reference",
                          "sample": f"{REF_SAMPLE_ROT} rotations per step (MEGADOCK CPU sources + FFTW-API shim, "
                                    f"OpenMP over all host cores)"},
@@ -483,6 +495,7 @@ def main():
     torch.cuda.set_stream(stream)
     with tempfile.TemporaryDirectory() as tmp:
         rp, lp = make_inputs(tmp)
+        config = workload_config(rp, lp)
         job = Job(["-R", rp, "-L", lp, "-F", str(N_FFT), "-t", str(T_POSES), "-D", "-o",
                    os.path.join(tmp, "bench.out")])
         rr, ri = job.receptor_grids()
@@ -612,9 +625,7 @@ def main():
         "metric": METRIC, "value": value, "unit": "rotations/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_batched, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": f"docking, {N_REC}/{N_LIG}-residue synthetic pair ({job.na_rec}/{job.na_lig} atoms), "
-                               f"N={N_FFT}, {ROT_SET} rotations, t={T_POSES}",
-                   "fft": N_FFT, "rotations": ROT_SET, "t": T_POSES, "rotations_per_launch": batch,
+        "config": {**config, "rotations_per_launch": batch,
                    "inverse_plane_plan": plan, "xline_tile": tile,
                    "l2": "working set per step >> L2 (54,000 rotations x ~25 MB of intermediates)",
                    "parallelism": f"replicas x{world}"},
