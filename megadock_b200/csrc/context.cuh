@@ -35,6 +35,7 @@ struct WorkSet {
     int *sstart = nullptr;      // [cap][N/2 + 2 kReach + 1]
     int2 *cq = nullptr;         // [cap][na]           charge entries bucketed by plane, atom order
     int *cstart = nullptr;      // [cap][N/2 + 1]
+    uint32_t *marks = nullptr;  // [cap][N/2][2][N/2 * words per row] core / surface marks (K0m -> K0)
 
     void release() {
         cudaFree(A);
@@ -47,24 +48,28 @@ struct WorkSet {
         cudaFree(sstart);
         cudaFree(cq);
         cudaFree(cstart);
+        cudaFree(marks);
         *this = WorkSet();
     }
     // Bytes of each buffer for launch groups of `cap` rotations.
+    static constexpr int kBufs = 11;
     struct Sizes {
-        size_t b[10];
+        size_t b[kBufs];
     };
     static Sizes need(size_t cap, size_t N, size_t t, size_t na) {
         const size_t NG = N / 2;
         return Sizes{{sizeof(float2) * cap * NG * N * N, sizeof(float2) * cap * N * (N / 2) * N,
                       sizeof(Cand) * cap * N * t, sizeof(uint32_t) * cap * NG * 2 * NG * ((NG + 31) / 32),
                       sizeof(int2) * cap * NG * NG * NG, sizeof(int) * cap * NG, sizeof(MarkEntry) * cap * na,
-                      sizeof(int) * cap * (NG + 2 * kReach + 1), sizeof(int2) * cap * na, sizeof(int) * cap * (NG + 1)}};
+                      sizeof(int) * cap * (NG + 2 * kReach + 1), sizeof(int2) * cap * na, sizeof(int) * cap * (NG + 1),
+                      sizeof(uint32_t) * cap * NG * 2 * NG * ((NG + 31) / 32)}};
     }
     cudaError_t allocate(const Sizes &z) {
         cudaError_t e = cudaSuccess;
-        void **slot[10] = {(void **)&A, (void **)&G, (void **)&cand, (void **)&vbits, (void **)&qlist,
-                           (void **)&qcount, (void **)&srec, (void **)&sstart, (void **)&cq, (void **)&cstart};
-        for (int k = 0; k < 10 && e == cudaSuccess; ++k) e = cudaMalloc(slot[k], z.b[k]);
+        void **slot[kBufs] = {(void **)&A,    (void **)&G,    (void **)&cand,   (void **)&vbits,
+                              (void **)&qlist, (void **)&qcount, (void **)&srec, (void **)&sstart,
+                              (void **)&cq,   (void **)&cstart, (void **)&marks};
+        for (int k = 0; k < kBufs && e == cudaSuccess; ++k) e = cudaMalloc(slot[k], z.b[k]);
         return e;
     }
 };
@@ -179,8 +184,9 @@ struct Sized {
         GridView G{c->ng, c->gw, (float)(c->ng * c->gw) / 2, c->d_gc, c->d_tw};
         LigandView L{c->na, c->d_atom, c->d_rad2, c->delta};
         k_atom_prep<NG><<<nb, kNTP, 0, s>>>(L, G, d_rot9, w.srec, w.sstart, w.cq, w.cstart);
-        k_vox_bits<NG><<<dim3(NG, nb), kNT0, 0, s>>>(L, G, w.srec, w.sstart, w.cq, w.cstart, w.vbits, w.qlist,
-                                                    w.qcount);
+        k_vox_mark<NG><<<dim3(NG, nb), kNT0, 0, s>>>(L, G, w.srec, w.sstart, w.marks);
+        k_vox_bits<NG, true><<<dim3(NG, nb), kNT0, 0, s>>>(L, G, w.srec, w.sstart, w.cq, w.cstart, w.vbits,
+                                                          w.qlist, w.qcount, w.marks);
     }
 
     // Voxel grids of nb rotations ([nb][ng^3] real, imaginary) into vr / vi.

@@ -355,11 +355,58 @@ __global__ void __launch_bounds__(kNTP)
 //    cells qlist[b][p][e] = (q * NG + s, sum as bits), qcount[b][p] entries.
 constexpr int kNT0 = 256;
 
+// K0m: the core and surface marks of one (rotation, x-plane i), computed once
+// per plane and stored for the K0 CTAs of planes i-2 .. i+2 (each of which
+// would otherwise mark its neighbour planes itself):
+//   marks[b][i][0] = core bits, marks[b][i][1] = surface bits (rows of W words).
+// Same tests and rounding as vox_mark, so the bits are the same.
 template <int NG>
+__global__ void __launch_bounds__(kNT0)
+    k_vox_mark(LigandView L, GridView G, const MarkEntry *__restrict__ rec, const int *__restrict__ sstart,
+               uint32_t *__restrict__ marks) {
+    constexpr int W = VoxShared<NG>::W;
+    constexpr int NBS = NG + 2 * kReach;
+    __shared__ uint32_t cs[2][NG * W];
+    const int i = blockIdx.x, b = blockIdx.y, tid = threadIdx.x;
+    for (int w = tid; w < 2 * NG * W; w += blockDim.x) (&cs[0][0])[w] = 0u;
+    __syncthreads();
+    const int ng = G.ng;
+    const int *ss = sstart + (size_t)b * (NBS + 1);
+    const int lo = ss[max(i - 2 + kReach, 0)], hi = ss[min(i + 2 + kReach + 1, NBS)];
+    const MarkEntry *rb = rec + (size_t)b * L.na;
+    for (int task = tid; task < (hi - lo) * 5; task += blockDim.x) {
+        const MarkEntry me = rb[lo + task / 5];
+        const int j = me.box.y - 2 + task % 5;
+        if (i >= ng || i < me.box.x - 2 || i > me.box.x + 2 || j < 0 || j >= ng) continue;
+        const float rc2 = me.pos.w, rs2 = __int_as_float(me.box.w);
+        const float d2 = __fadd_rn(sqdist(me.pos.x, __ldg(&G.gc[i])), sqdist(me.pos.y, __ldg(&G.gc[j])));
+        if (!(d2 < rc2)) continue;
+        const int ka = max(me.box.z - 2, 0), kb = min(me.box.z + 3, ng);
+        const int wb = ka >> 5;
+        unsigned long long cm = 0ull, sm = 0ull;
+        for (int k = ka; k < kb; ++k) {
+            const float d3 = __fadd_rn(d2, sqdist(me.pos.z, __ldg(&G.gc[k])));
+            const unsigned long long bit = 1ull << (k - 32 * wb);
+            if (d3 < rc2) cm |= bit;
+            if (d3 < rs2) sm |= bit;
+        }
+        uint32_t *crow = &cs[0][j * W + wb], *srow = &cs[1][j * W + wb];
+        if ((uint32_t)cm) atomicOr(crow, (uint32_t)cm);
+        if (cm >> 32) atomicOr(crow + 1, (uint32_t)(cm >> 32));
+        if ((uint32_t)sm) atomicOr(srow, (uint32_t)sm);
+        if (sm >> 32) atomicOr(srow + 1, (uint32_t)(sm >> 32));
+    }
+    __syncthreads();
+    uint32_t *dst = marks + ((size_t)b * NG + i) * 2 * NG * W;
+    for (int w = tid; w < 2 * NG * W; w += blockDim.x) dst[w] = (&cs[0][0])[w];
+}
+
+// PREMARKED: the marks come from K0m (marks != nullptr) instead of vox_mark.
+template <int NG, bool PREMARKED = false>
 __global__ void __launch_bounds__(kNT0)
     k_vox_bits(LigandView L, GridView G, const MarkEntry *__restrict__ rec, const int *__restrict__ sstart,
                const int2 *__restrict__ cq, const int *__restrict__ cstart, uint32_t *__restrict__ vbits,
-               int2 *__restrict__ qlist, int *__restrict__ qcount) {
+               int2 *__restrict__ qlist, int *__restrict__ qcount, const uint32_t *__restrict__ marks = nullptr) {
     constexpr int W = VoxShared<NG>::W;
     constexpr int NBS = NG + 2 * kReach;
     __shared__ VoxShared<NG> vs;
@@ -367,17 +414,35 @@ __global__ void __launch_bounds__(kNT0)
     __shared__ int first[NG * NG];
     __shared__ int count;
     const int p = blockIdx.x, b = blockIdx.y, tid = threadIdx.x;
-    for (int w = tid; w < 5 * NG * W; w += blockDim.x) (&vs.core[0][0])[w] = 0u;
-    for (int w = tid; w < 3 * NG * W; w += blockDim.x) (&vs.surf[0][0])[w] = 0u;
+    const bool gd = (L.delta != 1.0f);
+    if constexpr (PREMARKED) {
+        // core of planes p-2 .. p+2 (p-1 .. p+1 unless delta != 1, as vox_mark
+        // marks them), surface of p-1 .. p+1; planes outside the grid are 0
+        const uint32_t *mb = marks + (size_t)b * NG * 2 * NG * W;
+        for (int w = tid; w < 5 * NG * W; w += blockDim.x) {
+            const int slot = w / (NG * W), i = p - 2 + slot;
+            const bool on = (i >= 0 && i < G.ng && i < NG) && (gd || (slot >= 1 && slot <= 3));
+            (&vs.core[0][0])[w] = on ? mb[(size_t)i * 2 * NG * W + w % (NG * W)] : 0u;
+        }
+        for (int w = tid; w < 3 * NG * W; w += blockDim.x) {
+            const int i = p - 1 + w / (NG * W);
+            const bool on = (i >= 0 && i < G.ng && i < NG);
+            (&vs.surf[0][0])[w] = on ? mb[(size_t)i * 2 * NG * W + NG * W + w % (NG * W)] : 0u;
+        }
+    } else {
+        for (int w = tid; w < 5 * NG * W; w += blockDim.x) (&vs.core[0][0])[w] = 0u;
+        for (int w = tid; w < 3 * NG * W; w += blockDim.x) (&vs.surf[0][0])[w] = 0u;
+    }
     for (int w = tid; w < 2 * NG * W; w += blockDim.x) (&ob[0][0])[w] = 0u;
     for (int c = tid; c < NG * NG; c += blockDim.x) first[c] = 0x7fffffff;
     if (tid == 0) count = 0;
     __syncthreads();
-    const bool gd = (L.delta != 1.0f);
-    const int reach = gd ? 4 : 3;
-    const int *ss = sstart + (size_t)b * (NBS + 1);
-    const int lo = ss[max(p - reach + kReach, 0)], hi = ss[min(p + reach + kReach + 1, NBS)];
-    vox_mark<NG>(vs, rec + (size_t)b * L.na, lo, hi, G, p, gd);
+    if constexpr (!PREMARKED) {
+        const int reach = gd ? 4 : 3;
+        const int *ss = sstart + (size_t)b * (NBS + 1);
+        const int lo = ss[max(p - reach + kReach, 0)], hi = ss[min(p + reach + kReach + 1, NBS)];
+        vox_mark<NG>(vs, rec + (size_t)b * L.na, lo, hi, G, p, gd);
+    }
     for (int c = tid; c < NG * W; c += blockDim.x) {
         const int q = c / W, w = c % W;
         uint32_t c2, c1;

@@ -58,10 +58,10 @@ void release_work(md_ctx *c) {
 // Work sets holding at least `z` bytes per buffer.
 int ensure_bytes(md_ctx *ctx, const WorkSet::Sizes &z) {
     bool ok = true;
-    for (int k = 0; k < 10; ++k) ok = ok && z.b[k] <= ctx->have.b[k];
+    for (int k = 0; k < WorkSet::kBufs; ++k) ok = ok && z.b[k] <= ctx->have.b[k];
     if (ok) return MD_OK;
     WorkSet::Sizes m = ctx->have;
-    for (int k = 0; k < 10; ++k) m.b[k] = std::max(m.b[k], z.b[k]);
+    for (int k = 0; k < WorkSet::kBufs; ++k) m.b[k] = std::max(m.b[k], z.b[k]);
     const int cap = ctx->cap, t = ctx->cap_t, na = ctx->cap_na;
     release_work(ctx);
     for (auto &w : ctx->ws) MD_CUDA(w.allocate(m));
@@ -547,9 +547,10 @@ int md_dock_profile(md_ctx *ctx, const float *d_rot, int first_rot, int n_rot, i
     for (auto &e : ev) MD_CUDA(cudaEventCreate(&e));
     double acc[5] = {0, 0, 0, 0, 0};
     int nl = 0;
-    // atom prep, voxelizer, forward planes, x lines, one top-t pass per T poses, merge
+    // atom prep, marks, voxelizer, forward planes, x lines, one top-t pass per
+    // T poses, merge
     const int T = t == 1 ? 1 : (t <= 4 ? 4 : 16);
-    const int per_group = 5 + (t + T - 1) / T;
+    const int per_group = 6 + (t + T - 1) / T;
     for (int r = 0; r < n_rot; r += B) {
         const int nb = std::min(B, n_rot - r);
         MD_CUDA(cudaEventRecord(ev[0], ctx->stream));
@@ -593,7 +594,7 @@ int md_dock_pairs(md_ctx *runner, md_ctx *const *pairs, int npairs, const float 
         MD_CUDA(set_attrs(c->N));
         const int B = std::max(1, std::min(c->batch, std::max(n_rot[p], 1)));
         const WorkSet::Sizes zp = WorkSet::need(B, c->N, t, std::max(c->na, 1));
-        for (int k = 0; k < 10; ++k) z.b[k] = std::max(z.b[k], zp.b[k]);
+        for (int k = 0; k < WorkSet::kBufs; ++k) z.b[k] = std::max(z.b[k], zp.b[k]);
         key.insert(key.end(), {(uintptr_t)c, (uintptr_t)d_rotmat[p], (uintptr_t)n_rot[p], (uintptr_t)d_out[p],
                                (uintptr_t)B, (uintptr_t)c->na, (uintptr_t)c->N});
     }
