@@ -104,9 +104,12 @@ struct md_ctx {
     int batch = 1;
     int plan = 0;   // radix plan variant of the plane top-t kernel (C2RPlan)
     int tile = 32;  // kz lines per CTA of the x-line kernel (8, 16 or 32)
+    int lanes = kLanes;   // work sets / capture streams the batched graph alternates over (1 or 2)
     int cap = 0, cap_t = 0, cap_na = 0;
     WorkSet::Sizes have{};           // bytes held by each work-set buffer
     WorkSet ws[kLanes];
+    char *d_adj = nullptr;   // adjoint scratch (grows to the largest call)
+    size_t adj_cap = 0;
     // staging for host-buffer calls
     float *d_rot = nullptr;
     size_t rot_cap = 0;

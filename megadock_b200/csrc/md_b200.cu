@@ -51,6 +51,9 @@ void free_graphs(md_ctx *c) {
 void release_work(md_ctx *c) {
     free_graphs(c);
     for (auto &w : c->ws) w.release();
+    cudaFree(c->d_adj);
+    c->d_adj = nullptr;
+    c->adj_cap = 0;
     c->cap = c->cap_t = c->cap_na = 0;
     c->have = WorkSet::Sizes{};
 }
@@ -114,8 +117,9 @@ int run_dock(md_ctx *ctx, const float *d_rot, int first_rot, int n_rot, int t, D
         MD_CUDA(cudaGetLastError());
         return MD_OK;
     }
-    // batched form: the whole rotation loop as one captured CUDA graph; launch
-    // groups alternate between the two work sets and the two capture streams
+    // batched form: the whole rotation loop as one captured CUDA graph; with
+    // two lanes the launch groups alternate between the two work sets and the
+    // two capture streams, with one they run back to back on one stream
     auto key = std::make_tuple(first_rot, n_rot, t, B, d_rot, d_pose);
     auto it = ctx->graphs.find(key);
     if (it == ctx->graphs.end()) {
@@ -126,7 +130,7 @@ int run_dock(md_ctx *ctx, const float *d_rot, int first_rot, int n_rot, int t, D
         int group = 0;
         for (int r = 0; r < n_rot; r += B, ++group) {
             const int nb = std::min(B, n_rot - r);
-            const int lane = group % kLanes;
+            const int lane = group % ctx->lanes;
             launch_dock(ctx, lane, lane ? ctx->side : ctx->stream, d_rot + 9 * (size_t)r, nb, first_rot + r, t,
                         d_pose + (size_t)r * t);
         }
@@ -478,6 +482,15 @@ int md_release_work(md_ctx *ctx) {
     return MD_OK;
 }
 
+int md_set_lanes(md_ctx *ctx, int lanes) {
+    if (!ctx || lanes < 1 || lanes > kLanes) return MD_ERR_ARG;
+    if (lanes != ctx->lanes) {
+        free_graphs(ctx);
+        ctx->lanes = lanes;
+    }
+    return MD_OK;
+}
+
 int md_set_tile(md_ctx *ctx, int lines) {
     if (!ctx || (lines != 8 && lines != 16 && lines != 32)) return MD_ERR_ARG;
     if (lines != ctx->tile) {
@@ -651,33 +664,35 @@ int adjoint_core(md_ctx *ctx, const float *rotmat, int n, const int4 *shift, con
     const int B = std::max(1, std::min(ctx->batch, n));
     int rc = ensure_work(ctx, B, 1);
     if (rc) return rc;
-    float *d_rot = nullptr, *d_w = nullptr, *d_grad = nullptr, *d_vox = nullptr, *d_dq = nullptr, *d_lg = nullptr;
-    int4 *d_shift = nullptr;
-    int *d_sel = nullptr;
-    auto cleanup = [&]() {
-        cudaFree(d_rot);
-        cudaFree(d_w);
-        cudaFree(d_grad);
-        cudaFree(d_vox);
-        cudaFree(d_dq);
-        cudaFree(d_shift);
-        cudaFree(d_sel);
-        cudaFree(d_lg);
-    };
+    // device scratch, carved from one context buffer that only grows (no
+    // allocation per call once it is large enough)
+    const size_t sz[8] = {sizeof(float) * 9 * n,       sizeof(float) * n,
+                          sizeof(int4) * n,            sizeof(float) * 2 * ng3,
+                          sizeof(float) * 2 * ng3 * B, sizeof(float) * std::max(ctx->na, 1),
+                          sizeof(int) * std::max(n_lig, 1), sizeof(float) * 2 * ng3 * std::max(n_lig, 0)};
+    size_t off[8], total = 0;
+    for (int k = 0; k < 8; ++k) {
+        off[k] = total;
+        total += (sz[k] + 255) & ~size_t(255);
+    }
+    if (total > ctx->adj_cap) {
+        cudaFree(ctx->d_adj);
+        ctx->d_adj = nullptr;
+        ctx->adj_cap = 0;
+        MD_CUDA(cudaMalloc(&ctx->d_adj, total));
+        ctx->adj_cap = total;
+    }
+    char *base = ctx->d_adj;
+    float *d_rot = reinterpret_cast<float *>(base + off[0]), *d_w = reinterpret_cast<float *>(base + off[1]);
+    int4 *d_shift = reinterpret_cast<int4 *>(base + off[2]);
+    float *d_grad = reinterpret_cast<float *>(base + off[3]), *d_vox = reinterpret_cast<float *>(base + off[4]);
+    float *d_dq = reinterpret_cast<float *>(base + off[5]);
+    int *d_sel = reinterpret_cast<int *>(base + off[6]);
+    float *d_lg = reinterpret_cast<float *>(base + off[7]);
     cudaError_t e = cudaSuccess;
     auto step = [&](cudaError_t x) {
         if (e == cudaSuccess) e = x;
     };
-    step(cudaMalloc(&d_rot, sizeof(float) * 9 * n));
-    step(cudaMalloc(&d_w, sizeof(float) * n));
-    step(cudaMalloc(&d_shift, sizeof(int4) * n));
-    step(cudaMalloc(&d_grad, sizeof(float) * 2 * ng3));
-    step(cudaMalloc(&d_vox, sizeof(float) * 2 * ng3 * B));
-    step(cudaMalloc(&d_dq, sizeof(float) * std::max(ctx->na, 1)));
-    if (n_lig > 0) {
-        step(cudaMalloc(&d_sel, sizeof(int) * n_lig));
-        step(cudaMalloc(&d_lg, sizeof(float) * 2 * ng3 * n_lig));
-    }
     cudaStream_t s = ctx->stream;
     step(cudaMemcpyAsync(d_rot, rotmat, sizeof(float) * 9 * n, cudaMemcpyHostToDevice, s));
     step(cudaMemcpyAsync(d_w, w, sizeof(float) * n, cudaMemcpyHostToDevice, s));
@@ -685,7 +700,6 @@ int adjoint_core(md_ctx *ctx, const float *rotmat, int n, const int4 *shift, con
     step(cudaMemsetAsync(d_grad, 0, sizeof(float) * 2 * ng3, s));
     if (e != cudaSuccess) {
         ctx->err = std::string("adjoint: ") + cudaGetErrorString(e);
-        cleanup();
         return MD_ERR_CUDA;
     }
     const int thr = 256;
@@ -720,7 +734,6 @@ int adjoint_core(md_ctx *ctx, const float *rotmat, int n, const int4 *shift, con
         step(cudaMemcpyAsync(d_lig_i, d_lg + ng3 * n_lig, sizeof(float) * ng3 * n_lig, cudaMemcpyDeviceToHost, s));
     }
     step(cudaStreamSynchronize(s));
-    cleanup();
     if (e != cudaSuccess) {
         ctx->err = std::string("adjoint: ") + cudaGetErrorString(e);
         return MD_ERR_CUDA;
