@@ -108,8 +108,8 @@ struct md_ctx {
     int cap = 0, cap_t = 0, cap_na = 0;
     WorkSet::Sizes have{};           // bytes held by each work-set buffer
     WorkSet ws[kLanes];
-    char *d_adj = nullptr;   // adjoint scratch (grows to the largest call)
-    size_t adj_cap = 0;
+    char *d_scratch = nullptr;   // scratch of the adjoint and pose-scoring calls (grows to the largest call)
+    size_t scratch_cap = 0;
     // staging for host-buffer calls
     float *d_rot = nullptr;
     size_t rot_cap = 0;

@@ -51,9 +51,9 @@ void free_graphs(md_ctx *c) {
 void release_work(md_ctx *c) {
     free_graphs(c);
     for (auto &w : c->ws) w.release();
-    cudaFree(c->d_adj);
-    c->d_adj = nullptr;
-    c->adj_cap = 0;
+    cudaFree(c->d_scratch);
+    c->d_scratch = nullptr;
+    c->scratch_cap = 0;
     c->cap = c->cap_t = c->cap_na = 0;
     c->have = WorkSet::Sizes{};
 }
@@ -86,6 +86,28 @@ int ensure_work(md_ctx *ctx, int cap, int t) {
     ctx->cap = cap;
     ctx->cap_t = t;
     ctx->cap_na = na;
+    return MD_OK;
+}
+
+// Device scratch of the calls outside the docking graph (adjoint, pose
+// scores, pose terms): n sub-buffers of sz[k] bytes, 256-byte aligned, carved
+// from one context buffer that only grows, so repeated calls allocate nothing.
+int carve_scratch(md_ctx *ctx, const size_t *sz, int n, char **out) {
+    size_t off[16], total = 0;
+    if (n > 16) return MD_ERR_ARG;
+    for (int k = 0; k < n; ++k) {
+        off[k] = total;
+        total += (sz[k] + 255) & ~size_t(255);
+    }
+    if (total > ctx->scratch_cap) {
+        MD_CUDA(cudaStreamSynchronize(ctx->stream));
+        cudaFree(ctx->d_scratch);
+        ctx->d_scratch = nullptr;
+        ctx->scratch_cap = 0;
+        MD_CUDA(cudaMalloc(&ctx->d_scratch, total));
+        ctx->scratch_cap = total;
+    }
+    for (int k = 0; k < n; ++k) out[k] = ctx->d_scratch + off[k];
     return MD_OK;
 }
 
@@ -664,31 +686,18 @@ int adjoint_core(md_ctx *ctx, const float *rotmat, int n, const int4 *shift, con
     const int B = std::max(1, std::min(ctx->batch, n));
     int rc = ensure_work(ctx, B, 1);
     if (rc) return rc;
-    // device scratch, carved from one context buffer that only grows (no
-    // allocation per call once it is large enough)
     const size_t sz[8] = {sizeof(float) * 9 * n,       sizeof(float) * n,
                           sizeof(int4) * n,            sizeof(float) * 2 * ng3,
                           sizeof(float) * 2 * ng3 * B, sizeof(float) * std::max(ctx->na, 1),
                           sizeof(int) * std::max(n_lig, 1), sizeof(float) * 2 * ng3 * std::max(n_lig, 0)};
-    size_t off[8], total = 0;
-    for (int k = 0; k < 8; ++k) {
-        off[k] = total;
-        total += (sz[k] + 255) & ~size_t(255);
-    }
-    if (total > ctx->adj_cap) {
-        cudaFree(ctx->d_adj);
-        ctx->d_adj = nullptr;
-        ctx->adj_cap = 0;
-        MD_CUDA(cudaMalloc(&ctx->d_adj, total));
-        ctx->adj_cap = total;
-    }
-    char *base = ctx->d_adj;
-    float *d_rot = reinterpret_cast<float *>(base + off[0]), *d_w = reinterpret_cast<float *>(base + off[1]);
-    int4 *d_shift = reinterpret_cast<int4 *>(base + off[2]);
-    float *d_grad = reinterpret_cast<float *>(base + off[3]), *d_vox = reinterpret_cast<float *>(base + off[4]);
-    float *d_dq = reinterpret_cast<float *>(base + off[5]);
-    int *d_sel = reinterpret_cast<int *>(base + off[6]);
-    float *d_lg = reinterpret_cast<float *>(base + off[7]);
+    char *p[8];
+    if ((rc = carve_scratch(ctx, sz, 8, p))) return rc;
+    float *d_rot = reinterpret_cast<float *>(p[0]), *d_w = reinterpret_cast<float *>(p[1]);
+    int4 *d_shift = reinterpret_cast<int4 *>(p[2]);
+    float *d_grad = reinterpret_cast<float *>(p[3]), *d_vox = reinterpret_cast<float *>(p[4]);
+    float *d_dq = reinterpret_cast<float *>(p[5]);
+    int *d_sel = reinterpret_cast<int *>(p[6]);
+    float *d_lg = reinterpret_cast<float *>(p[7]);
     cudaError_t e = cudaSuccess;
     auto step = [&](cudaError_t x) {
         if (e == cudaSuccess) e = x;
@@ -855,16 +864,16 @@ int md_pose_scores(md_ctx *ctx, const float *rotmat, int n, const md_pose *poses
     }
     const int B = std::max(1, std::min(ctx->batch, n));
     if ((rc = ensure_work(ctx, B, 1))) return rc;
-    float *d_rot = nullptr, *d_vox = nullptr, *d_sc = nullptr;
-    int4 *d_shift = nullptr;
+    const size_t sz[4] = {sizeof(float) * 9 * n, sizeof(int4) * n, sizeof(float) * n, sizeof(float) * 2 * ng3 * B};
+    char *p[4];
+    if ((rc = carve_scratch(ctx, sz, 4, p))) return rc;
+    float *d_rot = reinterpret_cast<float *>(p[0]), *d_sc = reinterpret_cast<float *>(p[2]);
+    int4 *d_shift = reinterpret_cast<int4 *>(p[1]);
+    float *d_vox = reinterpret_cast<float *>(p[3]);
     cudaError_t e = cudaSuccess;
     auto step = [&](cudaError_t x) {
         if (e == cudaSuccess) e = x;
     };
-    step(cudaMalloc(&d_rot, sizeof(float) * 9 * n));
-    step(cudaMalloc(&d_shift, sizeof(int4) * n));
-    step(cudaMalloc(&d_sc, sizeof(float) * n));
-    step(cudaMalloc(&d_vox, sizeof(float) * 2 * ng3 * B));
     cudaStream_t s = ctx->stream;
     step(cudaMemcpyAsync(d_rot, rotmat, sizeof(float) * 9 * n, cudaMemcpyHostToDevice, s));
     step(cudaMemcpyAsync(d_shift, shift.data(), sizeof(int4) * n, cudaMemcpyHostToDevice, s));
@@ -879,10 +888,6 @@ int md_pose_scores(md_ctx *ctx, const float *rotmat, int n, const md_pose *poses
         step(cudaMemcpyAsync(scores, d_sc, sizeof(float) * n, cudaMemcpyDeviceToHost, s));
         step(cudaStreamSynchronize(s));
     }
-    cudaFree(d_rot);
-    cudaFree(d_shift);
-    cudaFree(d_sc);
-    cudaFree(d_vox);
     if (e != cudaSuccess) {
         ctx->err = std::string("pose scores: ") + cudaGetErrorString(e);
         return MD_ERR_CUDA;
