@@ -293,12 +293,16 @@ const SizedOps *sized_ops_a(int N);
 const SizedOps *sized_ops_b(int N);
 const SizedOps *sized_ops_c(int N);
 const SizedOps *sized_ops_d(int N);
+const SizedOps *sized_ops_e(int N);
+const SizedOps *sized_ops_f(int N);
 
 inline const SizedOps *sized_ops(int N) {
     if (const SizedOps *o = sized_ops_a(N)) return o;
     if (const SizedOps *o = sized_ops_b(N)) return o;
     if (const SizedOps *o = sized_ops_c(N)) return o;
-    return sized_ops_d(N);
+    if (const SizedOps *o = sized_ops_d(N)) return o;
+    if (const SizedOps *o = sized_ops_e(N)) return o;
+    return sized_ops_f(N);
 }
 
 }  // namespace mdb

@@ -227,24 +227,37 @@ struct Plan;
         static_assert(R1_ * R2_ == N_, "plan");                  \
     };
 MDB_PLAN(16, 4, 4)
+MDB_PLAN(18, 6, 3)
+MDB_PLAN(20, 4, 5)
+MDB_PLAN(22, 2, 11)
 MDB_PLAN(24, 4, 6)
+MDB_PLAN(28, 4, 7)
+MDB_PLAN(30, 6, 5)
 MDB_PLAN(32, 4, 8)
 MDB_PLAN(36, 4, 9)
 MDB_PLAN(40, 8, 5)
+MDB_PLAN(42, 6, 7)
+MDB_PLAN(44, 4, 11)
 MDB_PLAN(48, 4, 12)
 MDB_PLAN(50, 10, 5)
 MDB_PLAN(54, 6, 9)
 MDB_PLAN(56, 8, 7)
 MDB_PLAN(60, 4, 15)
 MDB_PLAN(64, 8, 8)
+MDB_PLAN(66, 6, 11)
+MDB_PLAN(70, 10, 7)
 MDB_PLAN(72, 8, 9)
 MDB_PLAN(80, 8, 10)
+MDB_PLAN(84, 12, 7)
+MDB_PLAN(88, 8, 11)
 MDB_PLAN(96, 8, 12)
 MDB_PLAN(100, 20, 5)
 MDB_PLAN(108, 12, 9)
 MDB_PLAN(112, 8, 14)
 MDB_PLAN(120, 8, 15)
 MDB_PLAN(128, 8, 16)
+MDB_PLAN(132, 12, 11)
+MDB_PLAN(140, 20, 7)
 MDB_PLAN(144, 12, 12)
 MDB_PLAN(160, 16, 10)
 #undef MDB_PLAN

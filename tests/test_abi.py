@@ -31,7 +31,7 @@ def test_cli_built(built):
 
 def test_kernel_sizes_built(built):
     from megadock_b200 import lib
-    for n in (32, 48, 64, 72, 80, 96, 100, 108, 112, 120, 128, 144, 160):
+    for n in (32, 36, 40, 44, 48, 56, 60, 64, 72, 80, 84, 88, 96, 100, 108, 112, 120, 128, 132, 140, 144, 160):
         assert lib().md_fft_size_supported(n) == 1
     for n in (90, 98, 2048):
         assert lib().md_fft_size_supported(n) == 0
@@ -49,6 +49,7 @@ def test_null_arguments_are_rejected(built):
     assert L.md_adjoint_poses(None, f, 1, None, f, f, f, f, None, 0, f, f) == E
     assert L.md_pose_scores(None, f, 1, None, f) == E
     assert L.md_release_work(None) == E
+    assert L.md_set_lanes(None, 1) == E
     assert L.md_pose_terms(None, f, f, 1, None, f) == E
     assert L.md_receptor_build(None, 1, f, f, f, f, -45.0, 1.0, 1.0, 1, f, f) == E
     assert L.md_job_receptor_to(None, None) == E

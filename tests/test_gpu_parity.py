@@ -44,6 +44,8 @@ def _setup(pairs, name, *extra):
     ("small", ("-F", "96", "-v", "0.9", "-r", "360")),
     ("small", ("-F", "80", "-r", "360")),
     ("small", ("-F", "160", "-r", "24")),
+    ("small", ("-F", "44", "-v", "2.5", "-r", "24")),
+    ("small", ("-F", "140", "-r", "24")),
 ])
 def test_device_voxels_bit_exact(built, gpu, pairs, name, extra):
     from megadock_b200 import rotation_matrix
@@ -76,7 +78,8 @@ def test_device_voxels_vs_reference(built, gpu, pairs):
 
 @pytest.mark.parametrize("name,extra", [("c0", ("-F", "96",)), ("c1", ("-F", "128",)), ("small", ("-F", "160",)),
                                         ("small", ("-F", "80",)), ("small", ("-F", "112",)),
-                                        ("small", ("-F", "48", "-v", "2.0"))])
+                                        ("small", ("-F", "48", "-v", "2.0")), ("small", ("-F", "88")),
+                                        ("small", ("-F", "132"))])
 def test_receptor_spectrum(built, gpu, pairs, name, extra):
     from oracle import oracle as O
     job, fp = _setup(pairs, name, *extra, "-r", "1")
@@ -122,6 +125,15 @@ def _check_rotation(got, rhat, job, r, t, m):
     ("small", ("-F", "112", "-r", "24"), 1, 6),
     ("small", ("-F", "120", "-r", "24"), 17, 3),
     ("small", ("-F", "144", "-r", "24"), 3, 4),
+    ("small", ("-F", "36", "-v", "3.0", "-r", "24"), 2, 4),
+    ("small", ("-F", "40", "-v", "3.0", "-r", "24"), 1, 4),
+    ("small", ("-F", "44", "-v", "2.5", "-r", "24"), 3, 4),
+    ("small", ("-F", "56", "-v", "2.0", "-r", "24"), 2, 4),
+    ("small", ("-F", "60", "-v", "2.0", "-r", "24"), 2, 4),
+    ("small", ("-F", "84", "-r", "24"), 3, 4),
+    ("small", ("-F", "88", "-r", "24"), 2, 4),
+    ("small", ("-F", "132", "-r", "24"), 3, 3),
+    ("small", ("-F", "140", "-r", "24"), 2, 3),
 ])
 def test_dock_matches_fp64_oracle(built, gpu, pairs, name, extra, t, nchk):
     from megadock_b200 import rotation_matrices
@@ -205,6 +217,28 @@ def test_batched_equals_plain(built, gpu, pairs):
         again = fp.cuda_fft(mats, t=3, first_rot=100)   # graph replay
         assert np.array_equal(plain, again)
     assert (plain["rot"].reshape(-1, 3) == (100 + np.arange(37))[:, None]).all()
+
+
+@pytest.mark.parametrize("extra", [("-F", "44", "-v", "2.5"), ("-F", "84"), ("-F", "132"), ("-F", "140")])
+def test_batched_forms_at_table_sizes(built, gpu, pairs, extra):
+    """The 11-smooth sizes: the batched graph (both lane counts, every tile)
+    returns the plain form's records bit for bit; the other radix plans agree
+    within twice the FP64 tolerance."""
+    from megadock_b200 import rotation_matrices
+    job, fp = _setup(pairs, "small", *extra, "-r", "360", "-t", "3")
+    mats = rotation_matrices(job.rotation_angles()[:40])
+    plain = fp.cuda_fft(mats, t=3).copy()
+    fp.set_batch(16)
+    for lanes in (2, 1):
+        fp.set_lanes(lanes)
+        for tile in (32, 16, 8):
+            fp.set_tile(tile)
+            assert np.array_equal(plain, fp.cuda_fft(mats, t=3)), (lanes, tile)
+    for plan in (1, 2):
+        fp.set_plan(plan)
+        got = fp.cuda_fft(mats, t=3).copy()
+        s0, s1 = plain["score"].astype(np.float64), got["score"].astype(np.float64)
+        assert np.all(np.abs(s1 - s0) <= 2 * (RTOL * np.abs(s0) + ATOL)), plan
 
 
 def test_zero_charge_and_single_atom(built, gpu, pairs):
