@@ -295,6 +295,8 @@ const SizedOps *sized_ops_c(int N);
 const SizedOps *sized_ops_d(int N);
 const SizedOps *sized_ops_e(int N);
 const SizedOps *sized_ops_f(int N);
+const SizedOps *sized_ops_g(int N);
+const SizedOps *sized_ops_h(int N);
 
 inline const SizedOps *sized_ops(int N) {
     if (const SizedOps *o = sized_ops_a(N)) return o;
@@ -302,7 +304,9 @@ inline const SizedOps *sized_ops(int N) {
     if (const SizedOps *o = sized_ops_c(N)) return o;
     if (const SizedOps *o = sized_ops_d(N)) return o;
     if (const SizedOps *o = sized_ops_e(N)) return o;
-    return sized_ops_f(N);
+    if (const SizedOps *o = sized_ops_f(N)) return o;
+    if (const SizedOps *o = sized_ops_g(N)) return o;
+    return sized_ops_h(N);
 }
 
 }  // namespace mdb

@@ -487,6 +487,7 @@ __global__ void __launch_bounds__(kNT1, 1)
     constexpr int NG = N / 2, OFF = N / 4, PITCH = N + 1;
     constexpr int R1 = Plan<N>::R1, R2 = Plan<N>::R2;
     constexpr int W = VoxShared<NG>::W;
+    constexpr bool PR = prune_ok<N>();
     extern __shared__ __align__(16) unsigned char smem_raw[];
     float2 *S = reinterpret_cast<float2 *>(smem_raw);   // N x PITCH
 
@@ -494,6 +495,11 @@ __global__ void __launch_bounds__(kNT1, 1)
     const int b = blockIdx.y;
     const int tid = threadIdx.x;
 
+    if constexpr (!PR && MODE != 2) {
+        // unpruned passes read the padding: make it zero
+        for (int c = tid; c < N * PITCH; c += blockDim.x) S[c] = make_float2(0.f, 0.f);
+        __syncthreads();
+    }
     if (MODE == 1) {
         for (int c = tid; c < NG * NG; c += blockDim.x) {
             const int q = c / NG, s = c % NG;
@@ -533,7 +539,7 @@ __global__ void __launch_bounds__(kNT1, 1)
     // z-FFT of the NG non-zero rows (lanes = rows, pruned columns)
     for (int it = tid; it < NG * R2; it += blockDim.x) {
         const int t = it / NG, q = it % NG;
-        fft_phase1<N, -1, true>(S + (q + OFF) * PITCH, 1, t, G.tw);
+        fft_phase1<N, -1, PR>(S + (q + OFF) * PITCH, 1, t, G.tw);
     }
     __syncthreads();
     {
@@ -559,7 +565,7 @@ __global__ void __launch_bounds__(kNT1, 1)
     // y-FFT of all N columns (lanes = columns, pruned rows); phase 2 -> global
     for (int it = tid; it < N * R2; it += blockDim.x) {
         const int t = it / N, c = it % N;
-        fft_phase1<N, -1, true>(S + c, PITCH, t, G.tw);
+        fft_phase1<N, -1, PR>(S + c, PITCH, t, G.tw);
     }
     __syncthreads();
     float2 *Ab = A + ((size_t)b * NG + p) * N * N;
@@ -601,11 +607,16 @@ __global__ void __launch_bounds__(kNT1B, 2)
     constexpr int NG = N / 2, OFF = N / 4, PZ = N + 1, CB = 32, PB = CB + 1;
     constexpr int R1 = Plan<N>::R1, R2 = Plan<N>::R2;
     constexpr int W = VoxShared<NG>::W;
-    static_assert(R1 % 4 == 0, "pruned y pass needs R1 % 4 == 0");
+    constexpr bool PR = prune_ok<N>();
     extern __shared__ __align__(16) unsigned char smem_raw[];
     float2 *Z = reinterpret_cast<float2 *>(smem_raw);   // NG rows x PZ
     float2 *Y = Z + NG * PZ;                             // N rows x PB
     const int p = blockIdx.x, b = blockIdx.y, tid = threadIdx.x;
+    if constexpr (!PR) {
+        // the unpruned z pass reads the padding columns: make them zero
+        for (int c = tid; c < NG * PZ; c += blockDim.x) Z[c] = make_float2(0.f, 0.f);
+        __syncthreads();
+    }
 
     // the plane's NG rows at column offset OFF (the pruned passes read no
     // other column)
@@ -628,7 +639,7 @@ __global__ void __launch_bounds__(kNT1B, 2)
     // z-FFT of the NG rows (lanes = rows, pruned columns)
     for (int it = tid; it < NG * R2; it += blockDim.x) {
         const int t = it / NG, q = it % NG;
-        fft_phase1<N, -1, true>(Z + q * PZ, 1, t, G.tw);
+        fft_phase1<N, -1, PR>(Z + q * PZ, 1, t, G.tw);
     }
     __syncthreads();
     {
@@ -660,10 +671,15 @@ __global__ void __launch_bounds__(kNT1B, 2)
             float2 v[R1];
             static_for<0, R1>([&](auto m_) {
                 constexpr int m = decltype(m_)::value;
-                if constexpr (m < R1 / 4 || m >= 3 * R1 / 4) {
-                    v[m] = make_float2(0.f, 0.f);
+                if constexpr (PR) {
+                    if constexpr (m < R1 / 4 || m >= 3 * R1 / 4) {
+                        v[m] = make_float2(0.f, 0.f);
+                    } else {
+                        v[m] = Z[(t + R2 * (m - R1 / 4)) * PZ + cb + c];   // row n - OFF, n = t + R2 m
+                    }
                 } else {
-                    v[m] = Z[(t + R2 * (m - R1 / 4)) * PZ + cb + c];   // row n - OFF, n = t + R2 m
+                    const int q = t + R2 * m - OFF;   // resident row of y = t + R2 m, if any
+                    v[m] = ((unsigned)q < (unsigned)NG) ? Z[q * PZ + cb + c] : make_float2(0.f, 0.f);
                 }
             });
             Dft<R1, -1>::run(v);
@@ -697,15 +713,20 @@ __global__ void __launch_bounds__(kNT)
     constexpr int R1 = Plan<N>::R1, R2 = Plan<N>::R2;
     constexpr int TILES = (N + kLT - 1) / kLT;
     __shared__ float2 X[N * kLT];
+    constexpr bool PR = prune_ok<N>();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
     const int ky = blockIdx.x / TILES;
     const int kz = (blockIdx.x % TILES) * kLT + lane;
     const bool ok = kz < N;
+    if constexpr (!PR) {
+        for (int c = threadIdx.x; c < N * kLT; c += blockDim.x) X[c] = make_float2(0.f, 0.f);
+        __syncthreads();
+    }
     for (int pp = warp; pp < NG; pp += nwarp)
         X[(pp + OFF) * kLT + lane] = ok ? A[((size_t)pp * N + ky) * N + kz] : make_float2(0.f, 0.f);
     __syncthreads();
     for (int it = threadIdx.x; it < kLT * R2; it += blockDim.x)
-        fft_phase1<N, -1, true>(X + (it % kLT), kLT, it / kLT, G.tw);
+        fft_phase1<N, -1, PR>(X + (it % kLT), kLT, it / kLT, G.tw);
     __syncthreads();
     for (int it = threadIdx.x; it < kLT * R1; it += blockDim.x) {
         const int ln = it % kLT, u = it / kLT;
@@ -746,7 +767,7 @@ __global__ void __launch_bounds__(16 * LT, xline_occ<N>() / LT)
     k_xline_herm(GridView G, const float2 *__restrict__ A, const float2 *__restrict__ Rh, float2 *__restrict__ Gh) {
     constexpr int NG = N / 2, NH = N / 2, OFF = N / 4;
     constexpr int R1 = Plan<N>::R1, R2 = Plan<N>::R2;
-    static_assert(R1 % 4 == 0, "pruned forward x pass needs R1 % 4 == 0");
+    constexpr bool PR = prune_ok<N>();
     constexpr int TILES = (N + LT - 1) / LT;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     float2 *X0 = reinterpret_cast<float2 *>(smem_raw);   // own tile   [N][LT]
@@ -773,11 +794,14 @@ __global__ void __launch_bounds__(16 * LT, xline_occ<N>() / LT)
             float2 v[R1];
             static_for<0, R1>([&](auto m_) {
                 constexpr int mm = decltype(m_)::value;
-                if constexpr (mm < R1 / 4 || mm >= 3 * R1 / 4) {
+                const int pp = t + R2 * mm - OFF;   // spectrum plane of x = t + R2 mm, if any
+                if constexpr (PR && (mm < R1 / 4 || mm >= 3 * R1 / 4)) {
                     v[mm] = make_float2(0.f, 0.f);
-                } else {
-                    const int pp = t + R2 * mm - OFF;
+                } else if constexpr (PR) {
                     v[mm] = ok ? Ab[((size_t)pp * N + row) * N + col] : make_float2(0.f, 0.f);
+                } else {
+                    v[mm] = (ok && (unsigned)pp < (unsigned)NG) ? Ab[((size_t)pp * N + row) * N + col]
+                                                                : make_float2(0.f, 0.f);
                 }
             });
             Dft<R1, -1>::run(v);

@@ -13,7 +13,10 @@
 //
 // Zero padding: docking grids carry data only in the middle half of each axis
 // ([N/4, 3N/4)).  With R1 % 4 == 0 the pruned phase 1 loads exactly
-// m in [R1/4, 3R1/4) for every t and skips the other (zero) inputs.
+// m in [R1/4, 3R1/4) for every t and skips the other (zero) inputs.  When
+// N/2 is odd (N % 4 == 2) the data sit at [floor(N/4), floor(N/4) + N/2) and no
+// split prunes evenly: those sizes run the unpruned phase 1 over explicit zeros
+// (prune_ok<N>() false).
 //
 // The small DFTs are generated at compile time: prime radices 2, 3, 5, 7, 11
 // are direct DFTs (radix 4 is a butterfly); composite radices recurse through
@@ -227,6 +230,9 @@ struct Plan;
         static_assert(R1_ * R2_ == N_, "plan");                  \
     };
 MDB_PLAN(16, 4, 4)
+MDB_PLAN(21, 3, 7)
+MDB_PLAN(25, 5, 5)
+MDB_PLAN(27, 3, 9)
 MDB_PLAN(18, 6, 3)
 MDB_PLAN(20, 4, 5)
 MDB_PLAN(22, 2, 11)
@@ -234,33 +240,54 @@ MDB_PLAN(24, 4, 6)
 MDB_PLAN(28, 4, 7)
 MDB_PLAN(30, 6, 5)
 MDB_PLAN(32, 4, 8)
+MDB_PLAN(33, 3, 11)
+MDB_PLAN(35, 5, 7)
 MDB_PLAN(36, 4, 9)
 MDB_PLAN(40, 8, 5)
 MDB_PLAN(42, 6, 7)
 MDB_PLAN(44, 4, 11)
+MDB_PLAN(45, 5, 9)
 MDB_PLAN(48, 4, 12)
+MDB_PLAN(49, 7, 7)
 MDB_PLAN(50, 10, 5)
 MDB_PLAN(54, 6, 9)
+MDB_PLAN(55, 5, 11)
 MDB_PLAN(56, 8, 7)
 MDB_PLAN(60, 4, 15)
+MDB_PLAN(63, 7, 9)
 MDB_PLAN(64, 8, 8)
 MDB_PLAN(66, 6, 11)
 MDB_PLAN(70, 10, 7)
 MDB_PLAN(72, 8, 9)
+MDB_PLAN(75, 5, 15)
+MDB_PLAN(77, 7, 11)
 MDB_PLAN(80, 8, 10)
 MDB_PLAN(84, 12, 7)
 MDB_PLAN(88, 8, 11)
+MDB_PLAN(90, 10, 9)
 MDB_PLAN(96, 8, 12)
+MDB_PLAN(98, 14, 7)
 MDB_PLAN(100, 20, 5)
 MDB_PLAN(108, 12, 9)
+MDB_PLAN(110, 10, 11)
 MDB_PLAN(112, 8, 14)
 MDB_PLAN(120, 8, 15)
+MDB_PLAN(126, 14, 9)
 MDB_PLAN(128, 8, 16)
 MDB_PLAN(132, 12, 11)
 MDB_PLAN(140, 20, 7)
 MDB_PLAN(144, 12, 12)
+MDB_PLAN(150, 10, 15)
+MDB_PLAN(154, 14, 11)
 MDB_PLAN(160, 16, 10)
 #undef MDB_PLAN
+
+// Whether the first passes of an axis of length N can skip the zero padding
+// (data in the middle half, split with R1 % 4 == 0).
+template <int N>
+constexpr bool prune_ok() {
+    return N % 4 == 0 && Plan<N>::R1 % 4 == 0;
+}
 
 // Phase 1 of one item on a line at `b` with element stride `es`.
 // tw: W_N^j = exp(-2*pi*i*j/N), j < N (forward table); S selects the sign.
