@@ -141,6 +141,29 @@ struct Sized {
     static constexpr int NH = N / 2;
     static constexpr int TILES = (N + kLT - 1) / kLT;
     static size_t smem_fwd() { return (size_t)N * (N + 1) * sizeof(float2); }
+    static size_t smem_xrec() { return (size_t)N * kLT * sizeof(float2); }
+    static size_t smem_vox() { return vox_bits_smem<NG>(); }
+    // the column-block forward form: always for MODE 0 where two CTAs fit, and
+    // for every mode where the one-CTA plane does not fit
+    template <int MODE>
+    static constexpr bool use_cb() {
+        return !fwd_full_fits<N>() || (MODE == 0 && fwd_cb_fits<N>());
+    }
+    template <int MODE, class Set>
+    static void set_fwd(Set &set) {
+        if constexpr (use_cb<MODE>()) set((const void *)k_plane_fwd_cb<N, MODE>, fwd_cb_smem<N>());
+        else set((const void *)k_plane_fwd<N, MODE>, smem_fwd());
+    }
+    template <int MODE>
+    static void plane_fwd(cudaStream_t s, int nb, const LigandView &L, const GridView &G, const uint32_t *vbits,
+                          const int2 *qlist, const int *qcount, const float *sr, const float *si, float2 *A,
+                          float *vr, float *vi) {
+        if constexpr (use_cb<MODE>())
+            k_plane_fwd_cb<N, MODE><<<dim3(NG, nb), kNT1B, fwd_cb_smem<N>(), s>>>(L, G, vbits, qlist, qcount, sr, si,
+                                                                                   A, vr, vi);
+        else
+            k_plane_fwd<N, MODE><<<dim3(NG, nb), kNT1, smem_fwd(), s>>>(L, G, vbits, qlist, qcount, sr, si, A, vr, vi);
+    }
     template <int LT = kLT>
     static size_t smem_xline() { return (size_t)2 * N * LT * sizeof(float2); }
     template <int V = 0>
@@ -156,10 +179,12 @@ struct Sized {
         auto set = [&](const void *f, size_t bytes) {
             if (e == cudaSuccess) e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
         };
-        set((const void *)k_plane_fwd<N, 0>, smem_fwd());
-        set((const void *)k_plane_fwd<N, 1>, smem_fwd());
-        set((const void *)k_plane_fwd<N, 2>, smem_fwd());
-        if constexpr (fwd_cb_fits<N>()) set((const void *)k_plane_fwd_cb<N>, fwd_cb_smem<N>());
+        set_fwd<0>(set);
+        set_fwd<1>(set);
+        set_fwd<2>(set);
+        set((const void *)k_xline_rec<N>, smem_xrec());
+        set((const void *)k_vox_bits<NG, true>, smem_vox());
+        set((const void *)k_vox_bits<NG, false>, smem_vox());
         set((const void *)k_xline_herm<N, 32>, smem_xline<32>());
         set((const void *)k_xline_herm<N, 16>, smem_xline<16>());
         set((const void *)k_xline_herm<N, 8>, smem_xline<8>());
@@ -177,9 +202,8 @@ struct Sized {
     static void receptor(md_ctx *c, const float *d_r, const float *d_i) {
         GridView G{c->ng, c->gw, 0.f, c->d_gc, c->d_tw};
         LigandView L{0, nullptr, nullptr, 1.f};
-        k_plane_fwd<N, 1><<<dim3(NG, 1), kNT1, smem_fwd(), c->stream>>>(L, G, nullptr, nullptr, nullptr, d_r, d_i,
-                                                                        c->ws[0].A, nullptr, nullptr);
-        k_xline_rec<N><<<dim3(N * TILES, 1), kNT, 0, c->stream>>>(G, c->ws[0].A, c->d_Rh);
+        plane_fwd<1>(c->stream, 1, L, G, nullptr, nullptr, nullptr, d_r, d_i, c->ws[0].A, nullptr, nullptr);
+        k_xline_rec<N><<<dim3(N * TILES, 1), kNT, smem_xrec(), c->stream>>>(G, c->ws[0].A, c->d_Rh);
     }
 
     // Voxelizer of one launch group (atom prep + K0).
@@ -188,8 +212,8 @@ struct Sized {
         LigandView L{c->na, c->d_atom, c->d_rad2, c->delta};
         k_atom_prep<NG><<<nb, kNTP, 0, s>>>(L, G, d_rot9, w.srec, w.sstart, w.cq, w.cstart);
         k_vox_mark<NG><<<dim3(NG, nb), kNT0, 0, s>>>(L, G, w.srec, w.sstart, w.marks);
-        k_vox_bits<NG, true><<<dim3(NG, nb), kNT0, 0, s>>>(L, G, w.srec, w.sstart, w.cq, w.cstart, w.vbits,
-                                                          w.qlist, w.qcount, w.marks);
+        k_vox_bits<NG, true><<<dim3(NG, nb), kNT0, smem_vox(), s>>>(L, G, w.srec, w.sstart, w.cq, w.cstart,
+                                                                   w.vbits, w.qlist, w.qcount, w.marks);
     }
 
     // Voxel grids of nb rotations ([nb][ng^3] real, imaginary) into vr / vi.
@@ -198,8 +222,7 @@ struct Sized {
         LigandView L{c->na, c->d_atom, c->d_rad2, c->delta};
         const WorkSet &w = c->ws[0];
         voxelize(c, w, d_rot9, nb, c->stream);
-        k_plane_fwd<N, 2><<<dim3(NG, nb), kNT1, smem_fwd(), c->stream>>>(L, G, w.vbits, w.qlist, w.qcount, nullptr,
-                                                                         nullptr, nullptr, d_vr, d_vi);
+        plane_fwd<2>(c->stream, nb, L, G, w.vbits, w.qlist, w.qcount, nullptr, nullptr, nullptr, d_vr, d_vi);
     }
 
     static void voxels(md_ctx *c, const float *d_rot9, float *d_vr, float *d_vi) {
@@ -207,8 +230,7 @@ struct Sized {
         LigandView L{c->na, c->d_atom, c->d_rad2, c->delta};
         const WorkSet &w = c->ws[0];
         voxelize(c, w, d_rot9, 1, c->stream);
-        k_plane_fwd<N, 2><<<dim3(NG, 1), kNT1, smem_fwd(), c->stream>>>(L, G, w.vbits, w.qlist, w.qcount, nullptr,
-                                                                        nullptr, nullptr, d_vr, d_vi);
+        plane_fwd<2>(c->stream, 1, L, G, w.vbits, w.qlist, w.qcount, nullptr, nullptr, nullptr, d_vr, d_vi);
     }
 
     // The plane top-t kernel in passes of T candidates (T = 1, 4 or 16), with
@@ -247,11 +269,7 @@ struct Sized {
         const float nf3f = (float)((long long)N * N * N);
         voxelize(c, w, d_rot9, nb, s);
         if (ev) cudaEventRecord(ev[1], s);
-        if constexpr (fwd_cb_fits<N>())
-            k_plane_fwd_cb<N><<<dim3(NG, nb), kNT1B, fwd_cb_smem<N>(), s>>>(L, G, w.vbits, w.qlist, w.qcount, w.A);
-        else
-            k_plane_fwd<N, 0><<<dim3(NG, nb), kNT1, smem_fwd(), s>>>(L, G, w.vbits, w.qlist, w.qcount, nullptr,
-                                                                    nullptr, w.A, nullptr, nullptr);
+        plane_fwd<0>(s, nb, L, G, w.vbits, w.qlist, w.qcount, nullptr, nullptr, w.A, nullptr, nullptr);
         if (ev) cudaEventRecord(ev[2], s);
         if (c->tile == 16)
             k_xline_herm<N, 16><<<dim3(NH * ((N + 15) / 16), nb), 256, smem_xline<16>(), s>>>(G, w.A, c->d_Rh, w.G);
@@ -297,6 +315,8 @@ const SizedOps *sized_ops_e(int N);
 const SizedOps *sized_ops_f(int N);
 const SizedOps *sized_ops_g(int N);
 const SizedOps *sized_ops_h(int N);
+const SizedOps *sized_ops_i(int N);
+const SizedOps *sized_ops_j(int N);
 
 inline const SizedOps *sized_ops(int N) {
     if (const SizedOps *o = sized_ops_a(N)) return o;
@@ -306,7 +326,9 @@ inline const SizedOps *sized_ops(int N) {
     if (const SizedOps *o = sized_ops_e(N)) return o;
     if (const SizedOps *o = sized_ops_f(N)) return o;
     if (const SizedOps *o = sized_ops_g(N)) return o;
-    return sized_ops_h(N);
+    if (const SizedOps *o = sized_ops_h(N)) return o;
+    if (const SizedOps *o = sized_ops_i(N)) return o;
+    return sized_ops_j(N);
 }
 
 }  // namespace mdb

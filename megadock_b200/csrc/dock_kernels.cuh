@@ -401,6 +401,12 @@ __global__ void __launch_bounds__(kNT0)
     for (int w = tid; w < 2 * NG * W; w += blockDim.x) dst[w] = (&cs[0][0])[w];
 }
 
+// Dynamic shared memory of k_vox_bits: the first charge entry of each cell.
+template <int NG>
+constexpr size_t vox_bits_smem() {
+    return sizeof(int) * NG * NG;
+}
+
 // PREMARKED: the marks come from K0m (marks != nullptr) instead of vox_mark.
 template <int NG, bool PREMARKED = false>
 __global__ void __launch_bounds__(kNT0)
@@ -411,8 +417,8 @@ __global__ void __launch_bounds__(kNT0)
     constexpr int NBS = NG + 2 * kReach;
     __shared__ VoxShared<NG> vs;
     __shared__ uint32_t ob[2][NG * W];
-    __shared__ int first[NG * NG];
     __shared__ int count;
+    extern __shared__ int first[];   // NG * NG (vox_bits_smem)
     const int p = blockIdx.x, b = blockIdx.y, tid = threadIdx.x;
     const bool gd = (L.delta != 1.0f);
     if constexpr (PREMARKED) {
@@ -588,10 +594,22 @@ __global__ void __launch_bounds__(kNT1, 1)
 // straight to global memory.
 constexpr int kNT1B = 512;
 
+constexpr size_t kSmemMax = 227 * 1024;   // dynamic shared memory one CTA may hold
+
+template <int N>
+constexpr size_t fwd_cb_smem_of(int cb) {
+    return ((size_t)(N / 2) * (N + 1) + (size_t)N * (cb + 1)) * sizeof(float2);
+}
+
+// Column-block width: 32 where it fits one CTA's shared memory, else 16 or 8.
+template <int N>
+constexpr int fwd_cb_width() {
+    return fwd_cb_smem_of<N>(32) <= kSmemMax ? 32 : (fwd_cb_smem_of<N>(16) <= kSmemMax ? 16 : 8);
+}
+
 template <int N>
 constexpr size_t fwd_cb_smem() {
-    constexpr int CB = 32;
-    return ((size_t)(N / 2) * (N + 1) + (size_t)N * (CB + 1)) * sizeof(float2);
+    return fwd_cb_smem_of<N>(fwd_cb_width<N>());
 }
 
 // two CTAs and their 1 KB system reservations within the SM's 228 KB
@@ -600,11 +618,21 @@ constexpr bool fwd_cb_fits() {
     return fwd_cb_smem<N>() <= 113 * 1024;
 }
 
+// whether the one-CTA form's N x (N+1) plane fits one CTA (N <= 168); larger
+// sizes run every mode in the column-block form
 template <int N>
-__global__ void __launch_bounds__(kNT1B, 2)
+constexpr bool fwd_full_fits() {
+    return (size_t)N * (N + 1) * sizeof(float2) <= kSmemMax;
+}
+
+// MODE as in k_plane_fwd: 0 ligand bits + charges, 1 receptor grids from
+// global, 2 the voxel plane itself (no FFT).
+template <int N, int MODE = 0>
+__global__ void __launch_bounds__(kNT1B, fwd_cb_fits<N>() ? 2 : 1)
     k_plane_fwd_cb(LigandView L, GridView G, const uint32_t *__restrict__ vbits, const int2 *__restrict__ qlist,
-                   const int *__restrict__ qcount, float2 *__restrict__ A) {
-    constexpr int NG = N / 2, OFF = N / 4, PZ = N + 1, CB = 32, PB = CB + 1;
+                   const int *__restrict__ qcount, const float *__restrict__ src_r, const float *__restrict__ src_i,
+                   float2 *__restrict__ A, float *__restrict__ vox_r, float *__restrict__ vox_i) {
+    constexpr int NG = N / 2, OFF = N / 4, PZ = N + 1, CB = fwd_cb_width<N>(), PB = CB + 1;
     constexpr int R1 = Plan<N>::R1, R2 = Plan<N>::R2;
     constexpr int W = VoxShared<NG>::W;
     constexpr bool PR = prune_ok<N>();
@@ -612,7 +640,7 @@ __global__ void __launch_bounds__(kNT1B, 2)
     float2 *Z = reinterpret_cast<float2 *>(smem_raw);   // NG rows x PZ
     float2 *Y = Z + NG * PZ;                             // N rows x PB
     const int p = blockIdx.x, b = blockIdx.y, tid = threadIdx.x;
-    if constexpr (!PR) {
+    if constexpr (!PR && MODE != 2) {
         // the unpruned z pass reads the padding columns: make them zero
         for (int c = tid; c < NG * PZ; c += blockDim.x) Z[c] = make_float2(0.f, 0.f);
         __syncthreads();
@@ -620,22 +648,41 @@ __global__ void __launch_bounds__(kNT1B, 2)
 
     // the plane's NG rows at column offset OFF (the pruned passes read no
     // other column)
-    const uint32_t *vb = vbits + ((size_t)b * NG + p) * 2 * NG * W;
-    for (int c = tid; c < NG * NG; c += blockDim.x) {
-        const int q = c / NG, s = c % NG;
-        const uint32_t bit = 1u << (s & 31);
-        const float v = (__ldg(&vb[q * W + (s >> 5)]) & bit) ? L.delta
-                        : (__ldg(&vb[NG * W + q * W + (s >> 5)]) & bit) ? 1.0f : 0.0f;
-        Z[q * PZ + s + OFF] = make_float2(v, 0.f);
+    if constexpr (MODE == 1) {
+        for (int c = tid; c < NG * NG; c += blockDim.x) {
+            const int q = c / NG, s = c % NG;
+            const size_t gidx = ((size_t)p * NG + q) * NG + s;
+            Z[q * PZ + s + OFF] = make_float2(src_r[gidx], src_i[gidx]);
+        }
+        __syncthreads();
+    } else {
+        const uint32_t *vb = vbits + ((size_t)b * NG + p) * 2 * NG * W;
+        for (int c = tid; c < NG * NG; c += blockDim.x) {
+            const int q = c / NG, s = c % NG;
+            const uint32_t bit = 1u << (s & 31);
+            const float v = (__ldg(&vb[q * W + (s >> 5)]) & bit) ? L.delta
+                            : (__ldg(&vb[NG * W + q * W + (s >> 5)]) & bit) ? 1.0f : 0.0f;
+            Z[q * PZ + s + OFF] = make_float2(v, 0.f);
+        }
+        __syncthreads();
+        const int nq = qcount[(size_t)b * NG + p];
+        const int2 *ql = qlist + ((size_t)b * NG + p) * NG * NG;
+        for (int e = tid; e < nq; e += blockDim.x) {
+            const int2 c = ql[e];
+            Z[(c.x / NG) * PZ + c.x % NG + OFF].y = __int_as_float(c.y);
+        }
+        __syncthreads();
+        if constexpr (MODE == 2) {
+            for (int c = tid; c < NG * NG; c += blockDim.x) {
+                const int q = c / NG, s = c % NG;
+                const float2 v = Z[q * PZ + s + OFF];
+                const size_t gidx = (((size_t)b * NG + p) * NG + q) * NG + s;
+                vox_r[gidx] = v.x;
+                vox_i[gidx] = v.y;
+            }
+            return;
+        }
     }
-    __syncthreads();
-    const int nq = qcount[(size_t)b * NG + p];
-    const int2 *ql = qlist + ((size_t)b * NG + p) * NG * NG;
-    for (int e = tid; e < nq; e += blockDim.x) {
-        const int2 c = ql[e];
-        Z[(c.x / NG) * PZ + c.x % NG + OFF].y = __int_as_float(c.y);
-    }
-    __syncthreads();
     // z-FFT of the NG rows (lanes = rows, pruned columns)
     for (int it = tid; it < NG * R2; it += blockDim.x) {
         const int t = it / NG, q = it % NG;
@@ -712,7 +759,8 @@ __global__ void __launch_bounds__(kNT)
     constexpr int NG = N / 2, OFF = N / 4;
     constexpr int R1 = Plan<N>::R1, R2 = Plan<N>::R2;
     constexpr int TILES = (N + kLT - 1) / kLT;
-    __shared__ float2 X[N * kLT];
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    float2 *X = reinterpret_cast<float2 *>(smem_raw);   // N x kLT
     constexpr bool PR = prune_ok<N>();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
     const int ky = blockIdx.x / TILES;
@@ -755,11 +803,11 @@ __global__ void __launch_bounds__(kNT)
 //
 // xline_occ: threads per SM the kernel is compiled for, in units of 16:
 // 1,280 where that register budget (51 per thread) holds the kernel without
-// spills, else 1,024.  B200, 13,824 rotations at 192 per launch: +2.0 % at
+// spills, 512 above N = 160 (radices up to 20 need the registers), else 1,024.  B200, 13,824 rotations at 192 per launch: +2.0 % at
 // N=96; with spills at N=112 and 128 it lost 2 % and 7 %.
 template <int N>
 constexpr int xline_occ() {
-    return (N == 32 || N == 64 || N == 72 || N == 80 || N == 96) ? 80 : 64;
+    return (N == 32 || N == 64 || N == 72 || N == 80 || N == 96) ? 80 : (N > 160 ? 32 : 64);
 }
 
 template <int N, int LT = kLT>
@@ -1006,6 +1054,8 @@ struct C2RPlan {
 template <int N, int T, int V = 0>
 constexpr int c2r_min_blocks() {
     using P = C2RPlan<N, V>;
+    constexpr size_t pitch = (size_t)N + (P::R1 > 8 ? P::R1 : 8);
+    if ((size_t)(N / 2) * pitch * 8 > 113 * 1024) return 1;   // one CTA per SM by shared memory
     return (T <= 4 && P::R1 <= 8 && P::R2 <= 16 && P::Q1 <= 8 && P::Q2 <= 16) ? 3 : 2;
 }
 

@@ -261,13 +261,16 @@ MDB_PLAN(70, 10, 7)
 MDB_PLAN(72, 8, 9)
 MDB_PLAN(75, 5, 15)
 MDB_PLAN(77, 7, 11)
+MDB_PLAN(81, 9, 9)
 MDB_PLAN(80, 8, 10)
 MDB_PLAN(84, 12, 7)
 MDB_PLAN(88, 8, 11)
 MDB_PLAN(90, 10, 9)
 MDB_PLAN(96, 8, 12)
 MDB_PLAN(98, 14, 7)
+MDB_PLAN(99, 9, 11)
 MDB_PLAN(100, 20, 5)
+MDB_PLAN(105, 7, 15)
 MDB_PLAN(108, 12, 9)
 MDB_PLAN(110, 10, 11)
 MDB_PLAN(112, 8, 14)
@@ -280,6 +283,18 @@ MDB_PLAN(144, 12, 12)
 MDB_PLAN(150, 10, 15)
 MDB_PLAN(154, 14, 11)
 MDB_PLAN(160, 16, 10)
+MDB_PLAN(162, 18, 9)
+MDB_PLAN(168, 12, 14)
+MDB_PLAN(176, 16, 11)
+MDB_PLAN(180, 12, 15)
+MDB_PLAN(192, 12, 16)
+MDB_PLAN(196, 14, 14)
+MDB_PLAN(198, 18, 11)
+MDB_PLAN(200, 20, 10)
+MDB_PLAN(210, 14, 15)
+MDB_PLAN(216, 12, 18)
+MDB_PLAN(220, 20, 11)
+MDB_PLAN(224, 16, 14)
 #undef MDB_PLAN
 
 // Whether the first passes of an axis of length N can skip the zero padding

@@ -141,7 +141,8 @@ void run_rotation(cudaStream_t s, const LigandView &L, const GridView &G, const 
     constexpr int NG = N / 2, NH = N / 2, TILES = (N + kLT - 1) / kLT;
     const float nf3f = (float)((long long)N * N * N);
     k_atom_prep<NG><<<1, kNTP, 0, s>>>(L, G, rot9, pr.srec, pr.sstart, pr.cq, pr.cstart);
-    k_vox_bits<NG><<<dim3(NG, 1), kNT0, 0, s>>>(L, G, pr.srec, pr.sstart, pr.cq, pr.cstart, vbits, qlist, qcount);
+    k_vox_bits<NG><<<dim3(NG, 1), kNT0, vox_bits_smem<NG>(), s>>>(L, G, pr.srec, pr.sstart, pr.cq, pr.cstart, vbits,
+                                                                 qlist, qcount);
     k_plane_fwd<N, 0><<<dim3(NG, 1), kNT1, Smem<N>::fwd(), s>>>(L, G, vbits, qlist, qcount, nullptr, nullptr, A,
                                                                nullptr, nullptr);
     k_xline_herm<N, kLT><<<dim3(NH * TILES, 1), 16 * kLT, Smem<N>::xline(), s>>>(G, A, Rh, Gsp);

@@ -31,7 +31,7 @@
 
 namespace mdb {
 
-constexpr int kRecMaxNg = 96;   // row masks are two 64-bit words
+constexpr int kRecMaxNg = 112;   // row masks are two 64-bit words; 16 B x 112^2 of shared memory
 
 struct RecAtom {
     float x, y, z;

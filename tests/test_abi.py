@@ -32,9 +32,10 @@ def test_cli_built(built):
 def test_kernel_sizes_built(built):
     from megadock_b200 import lib
     for n in (32, 36, 40, 44, 48, 56, 60, 64, 72, 80, 84, 88, 96, 100, 108, 112, 120, 128, 132, 140, 144, 160,
-              42, 50, 54, 66, 70, 90, 98, 110, 126, 150, 154):
+              42, 50, 54, 66, 70, 90, 98, 110, 126, 150, 154,
+              162, 168, 176, 180, 192, 196, 198, 200, 210, 216, 220, 224):
         assert lib().md_fft_size_supported(n) == 1
-    for n in (46, 162, 2048):
+    for n in (46, 230, 240, 2048):
         assert lib().md_fft_size_supported(n) == 0
 
 

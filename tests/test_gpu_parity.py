@@ -48,6 +48,8 @@ def _setup(pairs, name, *extra):
     ("small", ("-F", "140", "-r", "24")),
     ("small", ("-F", "50", "-v", "2.5", "-r", "24")),
     ("small", ("-F", "154", "-r", "24")),
+    ("small", ("-F", "162", "-r", "24")),
+    ("small", ("-F", "224", "-r", "24")),
 ])
 def test_device_voxels_bit_exact(built, gpu, pairs, name, extra):
     from megadock_b200 import rotation_matrix
@@ -81,7 +83,8 @@ def test_device_voxels_vs_reference(built, gpu, pairs):
 @pytest.mark.parametrize("name,extra", [("c0", ("-F", "96",)), ("c1", ("-F", "128",)), ("small", ("-F", "160",)),
                                         ("small", ("-F", "80",)), ("small", ("-F", "112",)),
                                         ("small", ("-F", "48", "-v", "2.0")), ("small", ("-F", "88")),
-                                        ("small", ("-F", "132")), ("small", ("-F", "90")), ("small", ("-F", "154"))])
+                                        ("small", ("-F", "132")), ("small", ("-F", "90")), ("small", ("-F", "154")),
+                                        ("small", ("-F", "192")), ("small", ("-F", "224"))])
 def test_receptor_spectrum(built, gpu, pairs, name, extra):
     from oracle import oracle as O
     job, fp = _setup(pairs, name, *extra, "-r", "1")
@@ -147,6 +150,12 @@ def _check_rotation(got, rhat, job, r, t, m):
     ("small", ("-F", "126", "-r", "24"), 2, 3),
     ("small", ("-F", "150", "-r", "24"), 2, 3),
     ("small", ("-F", "154", "-r", "24"), 3, 3),
+    ("small", ("-F", "162", "-r", "24"), 2, 2),
+    ("small", ("-F", "168", "-r", "24"), 1, 2),
+    ("small", ("-F", "176", "-r", "24"), 3, 2),
+    ("small", ("-F", "192", "-r", "24"), 2, 2),
+    ("small", ("-F", "210", "-r", "24"), 1, 2),
+    ("small", ("-F", "224", "-r", "24"), 3, 2),
 ])
 def test_dock_matches_fp64_oracle(built, gpu, pairs, name, extra, t, nchk):
     from megadock_b200 import rotation_matrices
@@ -233,7 +242,8 @@ def test_batched_equals_plain(built, gpu, pairs):
 
 
 @pytest.mark.parametrize("extra", [("-F", "44", "-v", "2.5"), ("-F", "84"), ("-F", "132"), ("-F", "140"),
-                                   ("-F", "50", "-v", "2.5"), ("-F", "110"), ("-F", "154")])
+                                   ("-F", "50", "-v", "2.5"), ("-F", "110"), ("-F", "154"), ("-F", "192"),
+                                   ("-F", "224")])
 def test_batched_forms_at_table_sizes(built, gpu, pairs, extra):
     """The 11-smooth sizes: the batched graph (both lane counts, every tile)
     returns the plain form's records bit for bit; the other radix plans agree
@@ -255,7 +265,7 @@ def test_batched_forms_at_table_sizes(built, gpu, pairs, extra):
         assert np.all(np.abs(s1 - s0) <= 2 * (RTOL * np.abs(s0) + ATOL)), plan
 
 
-@pytest.mark.parametrize("extra", [("-F", "90"), ("-F", "154"), ("-F", "132")])
+@pytest.mark.parametrize("extra", [("-F", "90"), ("-F", "154"), ("-F", "132"), ("-F", "224")])
 def test_direct_pose_scores_at_table_sizes(built, gpu, pairs, extra):
     """The direct-sum rescoring (md_pose_scores, the adjoint's shift
     convention) gives the docking scores at their poses: the embedding
@@ -300,8 +310,8 @@ def test_errors_are_status_codes(built, gpu):
         fp.cuda_fft(np.zeros((1, 9), np.float32))
     assert e.value.code == 3          # no grid yet
     with pytest.raises(MdError) as e:
-        fp.alloc_array(162, 1.2, np.zeros(81, np.float32))
-    assert e.value.code == 4          # no kernel set for N=162
+        fp.alloc_array(230, 1.2, np.zeros(115, np.float32))
+    assert e.value.code == 4          # no kernel set for N=230
     fp.alloc_array(64, 1.2, np.zeros(32, np.float32))
     with pytest.raises(MdError) as e:
         fp.ligand_data_transfer_gpu(np.zeros((40000, 3)), np.ones(40000), np.zeros(40000))

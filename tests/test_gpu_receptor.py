@@ -27,6 +27,8 @@ def _case(pairs, name, extra):
     ("small", ("-F", "96", "-v", "0.9"), -45.0, 1.0, 1.0),
     ("small", ("-F", "48", "-v", "2.0", "-d", "0"), -45.0, 0.0, 1.0),
     ("c0", ("-F", "160", "-e", "2.5"), -45.0, 1.0, 2.5),
+    ("c0", ("-F", "154"), -45.0, 1.0, 1.0),
+    ("c0", ("-F", "224"), -45.0, 1.0, 1.0),
 ])
 def test_device_receptor_grids_bit_exact(built, gpu, pairs, name, extra, core, acer, elec):
     job, fp, xyz_c, rad, q, ace = _case(pairs, name, extra)
