@@ -156,6 +156,15 @@ def _check_rotation(got, rhat, job, r, t, m):
     ("small", ("-F", "192", "-r", "24"), 2, 2),
     ("small", ("-F", "210", "-r", "24"), 1, 2),
     ("small", ("-F", "224", "-r", "24"), 3, 2),
+    ("small", ("-F", "72", "-r", "24"), 2, 3),
+    ("small", ("-F", "100", "-r", "24"), 3, 3),
+    ("small", ("-F", "108", "-r", "24"), 1, 3),
+    ("small", ("-F", "180", "-r", "24"), 2, 2),
+    ("small", ("-F", "196", "-r", "24"), 1, 2),
+    ("small", ("-F", "198", "-r", "24"), 3, 2),
+    ("small", ("-F", "200", "-r", "24"), 2, 2),
+    ("small", ("-F", "216", "-r", "24"), 1, 2),
+    ("small", ("-F", "220", "-r", "24"), 2, 2),
 ])
 def test_dock_matches_fp64_oracle(built, gpu, pairs, name, extra, t, nchk):
     from megadock_b200 import rotation_matrices
