@@ -41,9 +41,17 @@ constexpr size_t kScratchBytes = size_t(32) << 20;
 constexpr int kMaxN = 128;
 constexpr int kMaxT = 64;
 constexpr int kMaxDevices = 64;
-// twiddle tables for every supported N <= kMaxN, concatenated
-constexpr int kTwSizes[] = {32, 48, 64, 72, 80, 96, 100, 108, 112, 120, 128};
-constexpr int kTwTotal = 32 + 48 + 64 + 72 + 80 + 96 + 100 + 108 + 112 + 120 + 128;
+// every grid-table size N <= kMaxN
+#define MDB_NOALLOC_SIZES(X)                                                                                  \
+    X(32) X(36) X(40) X(42) X(44) X(48) X(50) X(54) X(56) X(60) X(64) X(66) X(70) X(72) X(80) X(84) X(88) \
+    X(90) X(96) X(98) X(100) X(108) X(110) X(112) X(120) X(126) X(128)
+// twiddle tables for every supported N, concatenated
+#define MDB_LIST(n) n,
+constexpr int kTwSizes[] = {MDB_NOALLOC_SIZES(MDB_LIST)};
+#undef MDB_LIST
+#define MDB_SUM(n) +n
+constexpr int kTwTotal = 0 MDB_NOALLOC_SIZES(MDB_SUM);
+#undef MDB_SUM
 
 static __device__ __align__(256) unsigned char g_scratch[kScratchBytes];
 static __device__ __align__(256) float2 g_twiddle[kTwTotal];
@@ -110,7 +118,7 @@ int setup(int dev) {
     cudaError_t e = cudaSuccess;
 #define X(n) \
     if (e == cudaSuccess) e = set_attrs<n>();
-    X(32) X(48) X(64) X(72) X(80) X(96) X(100) X(108) X(112) X(120) X(128)
+    MDB_NOALLOC_SIZES(X)
 #undef X
     if (e != cudaSuccess) return MD_ERR_CUDA;
     st.ready = true;
@@ -211,7 +219,7 @@ extern "C" int md_dock_noalloc(int nf1, float grid_width, const float *d_grid_co
         switch (nf1) {
 #define X(n) \
     case n: run_rotation<n>(s, L, G, rot9, Rh, prep, vbits, qlist, qcount, A, Gsp, cand, first_rot + r, t, pr); break;
-            X(32) X(48) X(64) X(72) X(80) X(96) X(100) X(108) X(112) X(120) X(128)
+            MDB_NOALLOC_SIZES(X)
 #undef X
         }
     }

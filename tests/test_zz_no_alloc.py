@@ -29,13 +29,15 @@ def _check(got, want):
         assert np.array_equal(got[f], want[f]), f
 
 
-def test_noalloc_matches_md_dock(built, gpu, pairs):
+@pytest.mark.parametrize("name,extra", [("c0", ("-F", "96", "-e", "0.06", "-t", "3")),
+                                        ("small", ("-F", "110", "-t", "2")), ("small", ("-F", "88", "-t", "1"))])
+def test_noalloc_matches_md_dock(built, gpu, pairs, name, extra):
     import torch
 
     from megadock_b200 import POSE_DTYPE, FFTProcess, Job, lib, rotation_matrices
 
-    rp, lp = pairs["c0"]
-    job = Job(["-R", rp, "-L", lp, "-F", "96", "-e", "0.06", "-r", "360", "-t", "3"])
+    rp, lp = pairs[name]
+    job = Job(["-R", rp, "-L", lp, "-r", "360", *extra])
     fp = FFTProcess(0)
     fp.alloc_array(job.nf1, job.grid_width, job.grid_coord())
     rr, ri = job.receptor_grids()
