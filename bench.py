@@ -626,7 +626,7 @@ def main():
         "warmup": args.warmup, "ms_per_step": ms_batched, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {**config, "rotations_per_launch": batch,
-                   "inverse_plane_plan": plan, "xline_tile": tile,
+                   "inverse_plane_plan": plan, "xline_tile": tile, "groups_in_flight": fp.lanes,
                    "l2": "working set per step >> L2 (54,000 rotations x ~25 MB of intermediates)",
                    "parallelism": f"replicas x{world}"},
         "plain": {"value": plain, "ms_per_step": ms_plain, "unit": "rotations/s",

@@ -87,6 +87,11 @@ int md_set_plan(md_ctx *ctx, int plan);
 /* Tile shape of the x-line kernel: 8, 16 or 32 kz lines per CTA (default
  * 32); also picked by the autotuner. */
 int md_set_tile(md_ctx *ctx, int lines);
+/* Launch groups of the batched form in flight at once: 2 (default) alternates
+ * them over two work sets and two streams so that one group's kernels overlap
+ * the next one's; 1 runs them back to back on one stream.  Which is faster
+ * depends on the size; the autotuner picks it. */
+int md_set_lanes(md_ctx *ctx, int lanes);
 
 /* FFTProcess::cuda_fft (src/fft_process.cpp:502-656) over rotations
  * [first_rot, first_rot + n_rot): rotate, voxelize, FFT, conj(R^) product,

@@ -49,6 +49,7 @@ _PROTOS = {
     "md_ligand_data": (C.c_int, [_VP, C.c_int, _FP, _FP, _FP, C.c_float]),
     "md_set_batch": (C.c_int, [_VP, C.c_int]),
     "md_release_work": (C.c_int, [_VP]),
+    "md_set_lanes": (C.c_int, [_VP, C.c_int]),
     "md_set_plan": (C.c_int, [_VP, C.c_int]),
     "md_set_tile": (C.c_int, [_VP, C.c_int]),
     "md_dock": (C.c_int, [_VP, _FP, C.c_int, C.c_int, C.c_int, _VP]),

@@ -34,7 +34,7 @@ class FFTProcess:
         self._h = h
         self.num_fft = 0
         self._top = None
-        self.plan, self.tile = 0, 32
+        self.plan, self.tile, self.lanes = 0, 32, 2
         if stream is not None:
             _check(N.lib().md_set_stream(self._h, C.c_void_p(stream)), self._h)
 
@@ -95,6 +95,11 @@ class FFTProcess:
         """kz lines per CTA of the x-line kernel (8, 16 or 32)."""
         _check(N.lib().md_set_tile(self._h, int(lines)), self._h)
         self.tile = int(lines)
+
+    def set_lanes(self, lanes: int):
+        """Launch groups of the batched form in flight at once (1 or 2)."""
+        _check(N.lib().md_set_lanes(self._h, int(lanes)), self._h)
+        self.lanes = int(lanes)
 
     def set_plan(self, plan: int):
         """Radix plan variant of the inverse plane kernel (0, 1 or 2)."""
