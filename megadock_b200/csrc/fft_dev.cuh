@@ -279,7 +279,7 @@ MDB_PLAN(126, 14, 9)
 MDB_PLAN(128, 8, 16)
 MDB_PLAN(132, 12, 11)
 MDB_PLAN(140, 20, 7)
-MDB_PLAN(144, 12, 12)
+MDB_PLAN(144, 16, 9)
 MDB_PLAN(150, 10, 15)
 MDB_PLAN(154, 14, 11)
 MDB_PLAN(160, 16, 10)
