@@ -43,6 +43,8 @@ T_POSES = 3
 ROT_SET = 54000
 METRIC = "rotations/sec at 128^3, 54k rot: batched vs plain fused, same GPU, 1e-4 tol"
 REF_SAMPLE_ROT = 360
+REF_GPU_SAMPLE_ROT = 3600
+SCIPY_SAMPLE_ROT = 64
 PLAIN_SAMPLE = 5400
 
 
@@ -133,6 +135,61 @@ def cpu_reference(rp, lp, nrot=REF_SAMPLE_ROT):
     return nrot / secs, cores, secs
 
 
+def cpu_production_fft(rp, lp, nrot=SCIPY_SAMPLE_ROT):
+    """The same pipeline on the host cores with a production FFT library:
+    voxel grids from the oracle's C restatement of the reference's CPU
+    voxelizer, scipy.fft complex64 transforms (pocketfft/ducc, workers = all
+    host cores), the conj(R^) product, the inverse transform and the
+    reference's top-t rules, over the first nrot rotations of the job."""
+    import numpy as np
+    import scipy.fft as sf
+
+    from megadock_b200 import Job, rotation_matrices
+    from oracle import oracle as O
+    job = Job(["-R", rp, "-L", lp, "-F", str(N_FFT), "-t", str(T_POSES), "-D"])
+    rr, ri = job.receptor_grids()
+    xyz, rad, q = job.ligand_atoms()
+    mats = rotation_matrices(job.rotation_angles()[:nrot])
+    gc = job.grid_coord()
+    cores = os.cpu_count() or 1
+    with sf.set_workers(cores):
+        rhat = O.receptor_spectrum(rr, ri, job.nf1, "fp32")
+        t0 = time.perf_counter()
+        for m in mats:
+            gr, gi = O.ligand_grids(O.rotate(xyz, m), rad, q, job.ng1, job.grid_width, gc, job.lig_core)
+            O.score_sort(O.raw_scores(rhat, gr, gi, "fp32"), T_POSES)
+        secs = time.perf_counter() - t0
+    return {"value": nrot / secs, "unit": "rotations/s", "cores": cores, "kind": "port",
+            "sample": f"first {nrot} rotations of the same job ({secs:.1f} s)",
+            "fft": f"scipy.fft (pocketfft) complex64, workers={cores}"}
+
+
+def gpu_reference(rp, lp, nrot=REF_GPU_SAMPLE_ROT):
+    """Time the reference's own GPU program (oracle/_ref/megadock-gpu-ref: its
+    CUDA path -- per-rotation voxelization kernels, cuFFT C2C transforms and
+    the block-maximum search, src/fft_process.cpp:502-807 -- built from its
+    sources for sm_100a) on nrot rotations of the same job, one host thread
+    driving the one GPU.  Rate = nrot / its "CPU time (docking)" line (wall
+    time of the rotation loop)."""
+    from oracle import ref
+    exe = ref.REF_BIN.parent / "megadock-gpu-ref"
+    if not exe.exists():
+        return {"unavailable": "oracle/_ref/megadock-gpu-ref was not built (needs the reference sources and cuFFT)"}
+    env = dict(os.environ, OMP_NUM_THREADS="1", MD_SHIM_FFT="fp32")
+    with tempfile.TemporaryDirectory() as d:
+        res = subprocess.run([str(exe), "-R", rp, "-L", lp, "-F", str(N_FFT), "-t", str(T_POSES), "-r", str(nrot),
+                              "-o", os.path.join(d, "gpu.out")], capture_output=True, text=True, env=env,
+                             timeout=900)
+    if res.returncode != 0:
+        return {"error": (res.stdout + res.stderr)[-300:]}
+    m = re.search(r"CPU time \(docking\)\s*=\s*([0-9.]+)", res.stdout)
+    secs = float(m.group(1))
+    return {"value": nrot / secs, "unit": "rotations/s", "seconds": secs,
+            "sample": f"{nrot} rotations (-r {nrot}) of the same job, N={N_FFT}, t={T_POSES}",
+            "what": "MEGADOCK's own GPU path (cuFFT, one host thread, one GPU), unmodified sources built for "
+                    "sm_100a; its t > 1 keeps one candidate per 512-cell block"}
+
+
 def run_reference_arm(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -162,10 +219,19 @@ def run_reference_arm(args):
                    "rate": f"rotations/s of the {REF_SAMPLE_ROT}-rotation sample, the per-rotation cost being "
                            f"independent of the rotation count"},
         "cpu_baseline": {"value": value, "unit": "rotations/s", "cores": cores, "kind": "reference",
+                         "fft": "project-written scalar FFTW-API shim (libfftw3f is not on the image)",
                          "sample": f"{REF_SAMPLE_ROT} rotations per step (MEGADOCK CPU sources + FFTW-API shim, "
                                    f"OpenMP over all host cores)"},
         "e2e": {"value": value, "unit": "rotations/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
+    try:
+        import torch
+        if torch.cuda.is_available():
+            with tempfile.TemporaryDirectory() as tmp:
+                rp, lp = make_inputs(tmp)
+                line["reference_gpu"] = gpu_reference(rp, lp)
+    except Exception as e:  # an extra comparator, never required
+        line["reference_gpu"] = {"error": str(e)[:200]}
     print(json.dumps(line, default=float))
 
 
@@ -472,6 +538,45 @@ def main():
     if args.workload == "fit":
         return run_fit_workload(args)
 
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        # one rank per GPU: run this same command under torch.distributed.run
+        import socket
+
+        from megadock_b200.shard import torchrun_command
+        with socket.socket() as sk:
+            sk.bind(("127.0.0.1", 0))
+            port = sk.getsockname()[1]
+        cmd = torchrun_command(str(Path(__file__).resolve()), sys.argv[1:], args.gpus, port)
+        raise SystemExit(subprocess.run(["timeout", "-k", "60", "1800", *cmd]).returncode)
+    return run_metric(args)
+
+
+def parity_vs_golden(poses):
+    """Check the records of the timed run (n_rot x t poses, rotation order)
+    against the reference's per-rotation top-3 of every 15th rotation
+    (tests/golden/bench_n128_D_t3_rot.npz, written by the reference's own CPU
+    code): largest relative score difference against its FP32 and FP64 FFT
+    paths and the number of equal cells."""
+    import numpy as np
+    path = ROOT / "tests" / "golden" / "bench_n128_D_t3_rot.npz"
+    if not path.exists():
+        return {"error": f"{path.name} missing"}
+    g = np.load(path)
+    rots = g["rot"]
+    rec = poses.reshape(-1, T_POSES)[rots]
+    score = rec["score"].astype(np.float64)
+    cell = np.stack([rec["i"], rec["j"], rec["k"]], -1)
+    rel32 = np.abs(score - g["score32"]) / np.abs(g["score32"])
+    rel64 = np.abs(score - g["score64"]) / np.abs(g["score64"])
+    ok_rot = bool((rec["rot"] == rots[:, None]).all())
+    return {"rotations_checked": int(len(rots)), "poses_checked": int(rec.size),
+            "max_rel_vs_reference_fp32": float(rel32.max()), "max_rel_vs_fp64": float(rel64.max()),
+            "within_1e-4": bool((rel32 <= 1e-4).all() and (rel64 <= 1e-4).all()),
+            "cells_equal": int((cell == g["cell32"]).all(-1).sum()), "rotation_indices_ok": ok_rot,
+            "source": "every 15th rotation of the 54,000 set, reference CPU code (FP32 FFT and FP64 FFT)"}
+
+
+def run_metric(args):
     import numpy as np
     import torch
 
@@ -484,15 +589,18 @@ def main():
         import datetime
 
         import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device(f"cuda:{local}"))
 
-    from megadock_b200 import FFTProcess, Job, rotation_matrices
+    from megadock_b200 import POSE_DTYPE, FFTProcess, Job, rotation_matrices
+    from megadock_b200.shard import gather_records, max_over_ranks, shard_range
     from megadock_b200.tune import autotune
 
     # a dedicated stream: the library captures CUDA graphs on it, which the
     # legacy default stream does not allow
     stream = torch.cuda.Stream(device=local)
     torch.cuda.set_stream(stream)
+    dev = f"cuda:{local}"
     with tempfile.TemporaryDirectory() as tmp:
         rp, lp = make_inputs(tmp)
         config = workload_config(rp, lp)
@@ -502,12 +610,15 @@ def main():
         xyz, rad, q = job.ligand_atoms()
         mats = rotation_matrices(job.rotation_angles())
         nrot = len(mats)
+        # this rank's block of the one job (the whole job at one GPU)
+        r0, r1 = shard_range(nrot, rank, world)
+        nloc = r1 - r0
         fp = FFTProcess(local, stream=stream.cuda_stream)
         fp.alloc_array(job.nf1, job.grid_width, job.grid_coord())
         fp.receptor_fft(rr, ri)
         fp.ligand_data_transfer_gpu(xyz, rad, q, job.lig_core)
-        d_rot = torch.from_numpy(mats).to(f"cuda:{local}")
-        d_pose = torch.zeros(nrot * T_POSES * 5, dtype=torch.int32, device=f"cuda:{local}")
+        d_rot = torch.from_numpy(np.ascontiguousarray(mats[r0:r1])).to(dev)
+        d_pose = torch.zeros(nloc * T_POSES * 5, dtype=torch.int32, device=dev)
 
         if args.batch:
             batch, plan = args.batch, args.plan
@@ -516,6 +627,7 @@ def main():
         else:
             batch, plan = autotune(fp, d_rot.data_ptr(), d_pose.data_ptr(), T_POSES)
         tile = fp.tile
+        merged = {}
 
         def timed(fn, steps, warmup):
             for _ in range(warmup):
@@ -533,55 +645,69 @@ def main():
             torch.cuda.synchronize()
             ms = e0.elapsed_time(e1)
             if dist:
-                t = torch.tensor([ms], device=f"cuda:{local}")
-                dist.all_reduce(t, op=dist.ReduceOp.MAX)
+                ms = max_over_ranks(ms, device=dev)
                 dist.barrier()
-                ms = float(t.item())
             return ms / steps
 
         def dev_step():
-            fp.dock_device(d_rot.data_ptr(), 0, nrot, T_POSES, d_pose.data_ptr())
+            fp.dock_device(d_rot.data_ptr(), r0, nloc, T_POSES, d_pose.data_ptr())
+            if dist:
+                # the job's exchange step: every rank's records, in rotation order
+                merged["all"] = gather_records(d_pose, nrot, T_POSES)
 
         # batched, device-resident inputs
         fp.set_batch(batch)
         with Clocks(local) as clk:
             ms_batched = timed(dev_step, args.steps, args.warmup)
+        all_rec = merged["all"] if dist else d_pose
+        poses_timed = all_rec.cpu().numpy().view(POSE_DTYPE).copy() if rank == 0 else None
         # plain form (one rotation per pipeline, no graph): its per-rotation
         # cost does not depend on the rotation count, so it is timed on the
-        # first PLAIN_SAMPLE rotations of the set
+        # first PLAIN_SAMPLE rotations of this rank's block
         fp.set_batch(1)
+        ns = min(PLAIN_SAMPLE, nloc)
 
         def plain_step():
-            fp.dock_device(d_rot.data_ptr(), 0, PLAIN_SAMPLE, T_POSES, d_pose.data_ptr())
+            fp.dock_device(d_rot.data_ptr(), r0, ns, T_POSES, d_pose.data_ptr())
 
-        ms_plain = timed(plain_step, args.steps, 1) * nrot / PLAIN_SAMPLE
-        # e2e through the C ABI with host buffers
+        ms_plain = timed(plain_step, args.steps, 1) * nloc / ns
+        # e2e through the C ABI with host buffers: receptor grids, ligand and
+        # this block's rotation matrices in, poses out; rank 0 gathers the
+        # records (host gather)
         fp.set_batch(batch)
-        host_rot = np.ascontiguousarray(mats)
+        host_rot = np.ascontiguousarray(mats[r0:r1])
 
         def e2e_step():
             fp.receptor_fft(rr, ri)
             fp.ligand_data_transfer_gpu(xyz, rad, q, job.lig_core)
-            fp.cuda_fft(host_rot, t=T_POSES)
+            out = fp.cuda_fft(host_rot, t=T_POSES, first_rot=r0)
+            if dist:
+                from megadock_b200.shard import gather_poses
+                gather_poses(out)
 
         for _ in range(args.warmup):
             e2e_step()
         torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
         t0 = time.perf_counter()
         for _ in range(args.steps):
             e2e_step()
         torch.cuda.synchronize()
         ms_e2e = 1000.0 * (time.perf_counter() - t0) / args.steps
         if dist:
-            t = torch.tensor([ms_e2e], device=f"cuda:{local}")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms_e2e = float(t.item())
+            ms_e2e = max_over_ranks(ms_e2e, device=dev)
         # per-stage profile of the batched form (events on the launch stream)
-        stage_ms, launches_prof = fp.dock_profile(d_rot.data_ptr(), 0, nrot, T_POSES, d_pose.data_ptr())
+        stage_ms, launches_prof = fp.dock_profile(d_rot.data_ptr(), r0, nloc, T_POSES, d_pose.data_ptr())
+        launches_all = launches_prof
+        if dist:
+            t_l = torch.tensor([launches_prof], dtype=torch.int64, device=dev)
+            dist.all_reduce(t_l)
+            launches_all = int(t_l.item())
         cufft = None
         if rank == 0 and not args.no_cufft:
             try:
-                cufft = cufft_comparator(fp, job, mats, rr, ri, d_pose, stream, args.steps, args.warmup)
+                cufft = cufft_comparator(fp, job, mats[r0:r1], rr, ri, d_pose, stream, args.steps, args.warmup)
             except Exception as e:  # a comparator, never required
                 cufft = {"error": str(e)[:200]}
         fp.fft_memory_free()
@@ -592,7 +718,7 @@ def main():
         return
 
     N3 = N_FFT ** 3
-    nb_launches = -(-nrot // batch)
+    nb_launches = -(-nloc // batch)
     # algorithmic DRAM bytes per rotation per stage (complex64 = 8 B, NG = N/2)
     NG = N_FFT // 2
     stage_bytes = {
@@ -617,32 +743,37 @@ def main():
     traffic_per_rotation = {"voxelize": 79.4e3, "plane_fwd": 7.55e6, "xline": 17.14e6, "plane_inv": 8.47e6,
                             "merge": 3.3e3}
     traffic = traffic_per_rotation[names[dom]] * batch if N_FFT == 128 else None
-    value = world * nrot / (ms_batched * 1e-3)
-    plain = world * nrot / (ms_plain * 1e-3)
-    e2e = world * nrot / (ms_e2e * 1e-3)
+    value = nrot / (ms_batched * 1e-3)
+    plain = nrot / (ms_plain * 1e-3)
+    e2e = nrot / (ms_e2e * 1e-3)
     model_bytes = 52 * N3
+    pipe_bytes = sum(stage_bytes.values())
     line = {
         "metric": METRIC, "value": value, "unit": "rotations/s", "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": ms_batched, "higher_is_better": True, "scaling": "weak",
+        "warmup": args.warmup, "ms_per_step": ms_batched, "higher_is_better": True, "scaling": "strong",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {**config, "rotations_per_launch": batch,
                    "inverse_plane_plan": plan, "xline_tile": tile, "groups_in_flight": fp.lanes,
                    "l2": "working set per step >> L2 (54,000 rotations x ~25 MB of intermediates)",
-                   "parallelism": f"replicas x{world}"},
+                   "parallelism": f"rotation shards x{world}" + (", NCCL all-gather of the records" if dist else "")},
         "plain": {"value": plain, "ms_per_step": ms_plain, "unit": "rotations/s",
-                  "sample": f"first {PLAIN_SAMPLE} rotations per step, scaled to {ROT_SET}"},
+                  "sample": f"first {ns} rotations of each rank's block per step, scaled to the block"},
         "batched_over_plain": value / plain,
         "e2e": {"value": e2e, "unit": "rotations/s", "ms_per_step": ms_e2e,
-                "h2d_bytes_per_step": int(rr.nbytes + ri.nbytes + mats.nbytes + xyz.nbytes + rad.nbytes + q.nbytes),
+                "h2d_bytes_per_step": int(world * (rr.nbytes + ri.nbytes + xyz.nbytes + rad.nbytes + q.nbytes)
+                                          + mats.nbytes),
                 "d2h_bytes_per_step": int(nrot * T_POSES * 20)},
         "roofline": {"bound": "hbm", "kernel": names[dom], "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
                      "stage_ms": {n: float(stage_ms[k]) for k, n in enumerate(names)}},
-        "pipeline_bytes_per_rotation": {"model_52N3": model_bytes, "this_pipeline": sum(stage_bytes.values())},
+        "pipeline_bytes_per_rotation": {"model_52N3": model_bytes, "this_pipeline": pipe_bytes},
         "pipeline_model": {"bytes_per_rotation": model_bytes,
                            "achieved_GBps": model_bytes * value / 1e9,
-                           "frac": model_bytes * value / 1e9 / peak},
-        "gpu_launches": int(args.steps * launches_prof),
+                           "frac": model_bytes * value / 1e9 / (peak * world)},
+        "pipeline_own_bytes": {"bytes_per_rotation": pipe_bytes, "achieved_GBps": pipe_bytes * value / 1e9,
+                               "frac": pipe_bytes * value / 1e9 / (peak * world)},
+        "parity": parity_vs_golden(poses_timed),
+        "gpu_launches": int(args.steps * launches_all),
         "clocks": clk.summary(),
     }
     if cufft is not None:
@@ -655,7 +786,11 @@ def main():
                     rp2, lp2 = make_inputs(tmp)
                     v, cores, secs = cpu_reference(rp2, lp2)
                 line["cpu_baseline"] = {"value": v, "unit": "rotations/s", "cores": cores, "kind": "reference",
+                                        "fft": "project-written scalar FFTW-API shim (libfftw3f is not on the image)",
                                         "sample": f"{REF_SAMPLE_ROT} rotations of the same job ({secs:.1f} s)"}
+                with tempfile.TemporaryDirectory() as tmp:
+                    rp2, lp2 = make_inputs(tmp)
+                    line["cpu_baseline"]["production_fft"] = cpu_production_fft(rp2, lp2)
         except Exception as e:  # the baseline is reported, never required
             line["cpu_baseline"] = {"error": str(e)[:200]}
     print(json.dumps(line, default=float))

@@ -128,7 +128,7 @@ int md_dock_profile(md_ctx *ctx, const float *d_rotmat, int first_rot, int n_rot
  * device: the rPSC/ACE real grid and the electrostatic grid of na receptor
  * atoms (coordinates centred on the receptor, radius, charge and ACE value
  * per atom; -a, -d and -e values), bit-exact with the reference's CPU code
- * for grids up to ng1 = 96.  make_receptor = 1 also makes them this
+ * for grids up to ng1 = 112.  make_receptor = 1 also makes them this
  * context's receptor (R^ for md_dock, and the grids for the adjoint), as
  * md_receptor_fft would; grid_r / grid_i (ng1^3 host floats, may be NULL)
  * receive a copy.  Needs md_set_grid. */
@@ -190,13 +190,16 @@ int md_ligand_voxels(md_ctx *ctx, const float *rotmat9, float *grid_r, float *gr
  * synchronisation are not allowed): every intermediate lives in one 32 MiB
  * file-scope device array that each device loading the library holds until
  * exit.  The caller passes all inputs and outputs as device pointers:
- * grid_coord (ng1), receptor_spectrum (nf1^3 complex, interleaved re/im, as
- * md_receptor_spectrum returns it), centred xyz (3*na), radius and charge (na),
+ * grid_coord (ng1), receptor_spectrum (nf1^3 complex as interleaved float
+ * pairs re, im; md_receptor_spectrum returns separate re and im arrays, which
+ * the caller interleaves), centred xyz (3*na), radius and charge (na),
  * rotmat (9*n_rot), out (n_rot*t poses).  Limits: nf1 <= 128 with a built
  * kernel set, na <= 32768, t <= 64 (else MD_ERR_SIZE); rotations run one per
  * pipeline on `stream` (a cudaStream_t, NULL = default).  The first call on a
  * device does the set-up with that device current: make it before any stream
- * capture.  All calls share the one scratch array: calls that overlap on the
+ * capture.  Every call looks the scratch address up again and repeats the
+ * set-up when it changed (after cudaDeviceReset, or in another driver
+ * context on that device).  All calls share the one scratch array: calls that overlap on the
  * GPU race, so the caller must serialise them.  Nothing is allocated, freed or
  * synchronised; the call returns once the work is enqueued. */
 int md_dock_noalloc(int nf1, float grid_width, const float *d_grid_coord, const float *d_receptor_spectrum, int na,

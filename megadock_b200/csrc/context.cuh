@@ -80,6 +80,12 @@ constexpr int kLanes = 2;
 
 struct md_ctx {
     int device = 0;
+    // Identity of this context's captured state for other contexts' graph
+    // caches: uid is never reused within the process (a later context at the
+    // same heap address gets a new one) and gen is bumped whenever a change
+    // invalidates this context's own captured graphs (free_graphs).
+    uint64_t uid = 0;
+    uint64_t gen = 0;
     cudaStream_t own = nullptr;
     cudaStream_t stream = nullptr;
     cudaStream_t side = nullptr;     // second capture stream of the batched form

@@ -1193,8 +1193,67 @@ __global__ void __launch_bounds__(kNT, c2r_min_blocks<N, T, V>())
             });
         }
     };
-    if (floor.idx >= 0) scan(std::true_type{});
-    else scan(std::false_type{});
+    if (out0 > 0) {
+        // a later pass of T (t > T): the floor from the earlier passes is in
+        // force (out0 > 0 with no floor returned above)
+        scan(std::true_type{});
+    } else {
+        // (2c) pass 2 in place: every item writes its scores back over the
+        // slots it read and keeps its thread's largest score.
+        float tmax = -INFINITY;   // fmaxf drops NaN keys, which are never selected
+        for (int it = tid; it < N * Q1; it += blockDim.x) {
+            const int z = it % N, u = it / N;
+            float2 o[Q2];
+            static_for<0, Q2>([&](auto n2_) {
+                constexpr int n2 = decltype(n2_)::value;
+                o[n2] = S[(u * Q2 + n2) * PITCH + z];
+            });
+            Dft<Q2, +1>::run(o);
+            static_for<0, Q2>([&](auto k2_) {
+                constexpr int k2 = decltype(k2_)::value;
+                S[(u * Q2 + k2) * PITCH + z] = o[k2];
+                tmax = fmaxf(tmax, fmaxf(o[k2].x, o[k2].y));
+            });
+        }
+        // Threshold: in each warp the nsel-th largest of its lanes' maxima is
+        // the key of nsel distinct cells of this plane, so the plane's nsel-th
+        // best key is at least that value; the largest such value over the
+        // warps bounds it too.  A cell below the bound cannot be among the
+        // plane's nsel best, so only cells at or above it enter the lists
+        // (equal keys still compete on the index inside the lists).
+        __shared__ float thr_w[kNT / 32];
+        {
+            const int lane = tid & 31, warp = tid >> 5;
+            float v = tmax, thw = -INFINITY;
+            for (int r = 0; r < nsel; ++r) {
+                float m = v;
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+                thw = m;
+                const unsigned holders = __ballot_sync(0xffffffffu, v == m);
+                if (lane == __ffs(holders) - 1) v = -INFINITY;
+            }
+            if (lane == 0) thr_w[warp] = thw;
+        }
+        __syncthreads();
+        float thr = thr_w[0];
+        for (int w = 1; w < (int)(blockDim.x >> 5); ++w) thr = fmaxf(thr, thr_w[w]);
+        // the few threads holding a score at or above the bound insert theirs
+        // (each thread reads back only the slots it wrote)
+        if (tmax >= thr) {
+            for (int it = tid; it < N * Q1; it += blockDim.x) {
+                const int z = it % N, u = it / N;
+                const int cell0 = base + 2 * u * N + z;
+                static_for<0, Q2>([&](auto k2_) {
+                    constexpr int k2 = decltype(k2_)::value;
+                    constexpr int step = 2 * Q1 * k2 * N;
+                    const float2 s = S[(u * Q2 + k2) * PITCH + z];
+                    if (s.x >= thr) top.template insert<false>(s.x, cell0 + step, floor);
+                    if (s.y >= thr) top.template insert<false>(s.y, cell0 + step + N, floor);
+                });
+            }
+        }
+    }
     // merge: each warp takes its best nsel from its lanes' lists (shuffles
     // only), then warp 0 takes the plane's best nsel from the warps' lists,
     // with one block barrier in between
@@ -1218,11 +1277,17 @@ __global__ void __launch_bounds__(kNT, c2r_min_blocks<N, T, V>())
         owner = __shfl_sync(0xffffffffu, owner, 0);
         return c;
     };
-    for (int r = 0; r < nsel; ++r) {
-        int owner;
-        const Cand c = warp_best(top.head(), owner);
-        if (lane == 0) wl[warp][r] = c;
-        if (c.idx >= 0 && lane == owner) top.pop();
+    if (__any_sync(0xffffffffu, top.i[0] != INT_MAX)) {
+        for (int r = 0; r < nsel; ++r) {
+            int owner;
+            const Cand c = warp_best(top.head(), owner);
+            if (lane == 0) wl[warp][r] = c;
+            if (c.idx >= 0 && lane == owner) top.pop();
+        }
+    } else if (lane < nsel) {
+        // no lane of this warp holds a candidate (the common case below the
+        // plane's threshold): its list is empty
+        wl[warp][lane] = Cand{0.f, -1};
     }
     __syncthreads();
     if (warp == 0) {

@@ -14,7 +14,12 @@
 #include "adjoint_kernels.cuh"
 #include "receptor_kernels.cuh"
 
+#include <atomic>
+
 namespace {
+
+// md_dock_pairs graphs kept per runner context before the cache is emptied
+constexpr size_t kMaxPairGraphs = 32;
 
 bool size_supported(int N) { return sized_ops(N) != nullptr; }
 
@@ -42,6 +47,7 @@ void launch_dock(md_ctx *c, int lane, cudaStream_t s, const float *rot, int nb, 
 }
 
 void free_graphs(md_ctx *c) {
+    ++c->gen;   // graphs of md_dock_pairs that captured this context's arguments no longer match
     for (auto &kv : c->graphs) cudaGraphExecDestroy(kv.second);
     c->graphs.clear();
     for (auto &kv : c->pair_graphs) cudaGraphExecDestroy(kv.second);
@@ -188,8 +194,10 @@ int md_ctx_create(int device, md_ctx **out) {
     int n = 0;
     if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) return MD_ERR_CUDA;
     if (device < 0 || device >= n) return MD_ERR_ARG;
+    static std::atomic<uint64_t> next_uid{1};
     md_ctx *ctx = new md_ctx;
     ctx->device = device;
+    ctx->uid = next_uid.fetch_add(1);
     if (cudaSetDevice(device) != cudaSuccess ||
         cudaStreamCreateWithFlags(&ctx->own, cudaStreamNonBlocking) != cudaSuccess ||
         cudaStreamCreateWithFlags(&ctx->side, cudaStreamNonBlocking) != cudaSuccess ||
@@ -309,7 +317,7 @@ int md_receptor_build(md_ctx *ctx, int na, const float *xyz_centred, const float
     }
     const int ng = ctx->ng;
     if (ng > kRecMaxNg) {
-        ctx->err = "receptor grids on the device are built for ng1 <= 96";
+        ctx->err = "receptor grids on the device are built for ng1 <= " + std::to_string(kRecMaxNg);
         return MD_ERR_SIZE;
     }
     MD_CUDA(cudaSetDevice(ctx->device));
@@ -631,13 +639,21 @@ int md_dock_pairs(md_ctx *runner, md_ctx *const *pairs, int npairs, const float 
         const int B = std::max(1, std::min(c->batch, std::max(n_rot[p], 1)));
         const WorkSet::Sizes zp = WorkSet::need(B, c->N, t, std::max(c->na, 1));
         for (int k = 0; k < WorkSet::kBufs; ++k) z.b[k] = std::max(z.b[k], zp.b[k]);
-        key.insert(key.end(), {(uintptr_t)c, (uintptr_t)d_rotmat[p], (uintptr_t)n_rot[p], (uintptr_t)d_out[p],
-                               (uintptr_t)B, (uintptr_t)c->na, (uintptr_t)c->N});
+        // the pair's (uid, gen) stands for every argument the capture takes
+        // from it: grid width, core value, atom count, plan, tile and buffers
+        key.insert(key.end(), {(uintptr_t)c->uid, (uintptr_t)c->gen, (uintptr_t)d_rotmat[p], (uintptr_t)n_rot[p],
+                               (uintptr_t)d_out[p], (uintptr_t)B, (uintptr_t)c->na, (uintptr_t)c->N});
     }
     int rc = ensure_bytes(ctx, z);
     if (rc) return rc;
     auto it = ctx->pair_graphs.find(key);
     if (it == ctx->pair_graphs.end()) {
+        // keys of changed or destroyed pair contexts never match again: bound the cache
+        if (ctx->pair_graphs.size() >= kMaxPairGraphs) {
+            MD_CUDA(cudaStreamSynchronize(ctx->stream));
+            for (auto &kv : ctx->pair_graphs) cudaGraphExecDestroy(kv.second);
+            ctx->pair_graphs.clear();
+        }
         cudaGraph_t g;
         MD_CUDA(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
         cudaEventRecord(ctx->fork, ctx->stream);

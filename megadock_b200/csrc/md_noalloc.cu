@@ -19,7 +19,9 @@
 //   - rotations run one per fused pipeline (the plain form);
 //   - the first call on each device does the set-up (symbol address lookup,
 //     twiddle tables, kernel attributes) with that device current; make that
-//     first call before any stream capture;
+//     first call before any stream capture.  Every call looks the scratch
+//     address up again (a cheap host query) and repeats the set-up when it
+//     changed, as after cudaDeviceReset or in another driver context;
 //   - every call shares the one scratch array, which keeps the last call's
 //     contents: calls that overlap on the GPU (other streams, other threads)
 //     race and must be serialised by the caller.  No scratch region needs
@@ -97,13 +99,16 @@ cudaError_t set_attrs() {
     return e;
 }
 
-// Once per device, with that device current.
+// With the device current: the set-up, done again whenever the scratch
+// array's address differs from the one the set-up used (a reset device or a
+// different driver context loads the module's arrays anew).
 int setup(int dev) {
     std::lock_guard<std::mutex> lk(g_mu);
     DevState &st = g_state[dev];
-    if (st.ready) return MD_OK;
     void *p = nullptr;
     if (cudaGetSymbolAddress(&p, g_scratch) != cudaSuccess) return MD_ERR_CUDA;
+    if (st.ready && st.scratch == p) return MD_OK;
+    st.ready = false;
     st.scratch = static_cast<unsigned char *>(p);
     if (cudaGetSymbolAddress(&p, g_twiddle) != cudaSuccess) return MD_ERR_CUDA;
     st.twiddle = static_cast<float2 *>(p);

@@ -16,7 +16,7 @@ converted to float, which is what ``np.float32(float(text))`` does.  The table
 files keep the decimal text; their readers convert the same way.  Where a key
 occurs more than once, the first occurrence wins (std::map::insert semantics).
 
-Usage:  python extract_tables.py [path/to/reference/src]
+Usage:  python extract_tables.py <path to the MEGADOCK src directory>
 """
 import re
 import sys
@@ -112,4 +112,6 @@ def main(src):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference/src")
+    if len(sys.argv) != 2:
+        raise SystemExit("usage: python extract_tables.py <MEGADOCK src directory>")
+    main(sys.argv[1])

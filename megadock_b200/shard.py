@@ -36,6 +36,47 @@ def gather_poses(local: np.ndarray, group=None):
     return np.concatenate([np.frombuffer(b, POSE_DTYPE) for b in out])
 
 
+def gather_records(local, nrot: int, t: int, group=None):
+    """Every rank's block of pose records (an int32 tensor of n_local x t x 5
+    words: score bits, rotation, i, j, k, the md_pose layout, for the block
+    shard_range(nrot, rank, world)) concatenated in rotation order, on every
+    rank: one all-gather of equal-size padded blocks over the group's backend
+    (NCCL on the GPUs, gloo on the CPU).  This is the exchange step of a
+    sharded job, the gather of MEGADOCK's per-rotation records."""
+    import torch
+    import torch.distributed as dist
+    world = dist.get_world_size(group)
+    words = t * 5
+    block = -(-nrot // world) * words
+    buf = torch.zeros(block, dtype=torch.int32, device=local.device)
+    buf[:local.numel()] = local.reshape(-1)
+    parts = [torch.empty_like(buf) for _ in range(world)]
+    dist.all_gather(parts, buf, group=group)
+    out = []
+    for r in range(world):
+        r0, r1 = shard_range(nrot, r, world)
+        out.append(parts[r][:(r1 - r0) * words])
+    return torch.cat(out)
+
+
+def max_over_ranks(value: float, device=None, group=None) -> float:
+    """The largest value over the ranks of the group (timings: a sharded job
+    ends when its slowest rank does)."""
+    import torch
+    import torch.distributed as dist
+    v = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(v, op=dist.ReduceOp.MAX, group=group)
+    return float(v.item())
+
+
+def torchrun_command(script: str, argv: list[str], nproc: int, port: int) -> list[str]:
+    """Command that runs `script argv` as nproc ranks on this node, one per
+    GPU (torch.distributed.run, rendezvous on 127.0.0.1)."""
+    import sys
+    return [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={nproc}",
+            "--master-addr", "127.0.0.1", f"--master-port={port}", script, *argv]
+
+
 def _gpu_dock(job: Job, mats: np.ndarray, r0: int, r1: int, device: int, batch: int | None):
     fp = FFTProcess(device)
     fp.alloc_array(job.nf1, job.grid_width, job.grid_coord())

@@ -29,15 +29,27 @@ def _check(got, want):
         assert np.array_equal(got[f], want[f]), f
 
 
+@pytest.fixture(scope="module")
+def big_ligand(tmp_path_factory):
+    """A pair whose ligand has close to the 32,768-atom limit."""
+    from megadock_b200 import synth
+    return synth.write_pair(str(tmp_path_factory.mktemp("big")), 40, 3900, 77, stem="big")
+
+
 @pytest.mark.parametrize("name,extra", [("c0", ("-F", "96", "-e", "0.06", "-t", "3")),
-                                        ("small", ("-F", "110", "-t", "2")), ("small", ("-F", "88", "-t", "1"))])
-def test_noalloc_matches_md_dock(built, gpu, pairs, name, extra):
+                                        ("small", ("-F", "110", "-t", "2")), ("small", ("-F", "88", "-t", "1")),
+                                        # t > 16: several top-t passes of the plane kernel per rotation
+                                        ("small", ("-F", "64", "-t", "20")),
+                                        ("big", ("-F", "128", "-v", "2.0", "-t", "3"))])
+def test_noalloc_matches_md_dock(built, gpu, pairs, big_ligand, name, extra):
     import torch
 
     from megadock_b200 import POSE_DTYPE, FFTProcess, Job, lib, rotation_matrices
 
-    rp, lp = pairs[name]
+    rp, lp = big_ligand if name == "big" else pairs[name]
     job = Job(["-R", rp, "-L", lp, "-r", "360", *extra])
+    if name == "big":
+        assert 30000 < job.na_lig <= 32768, job.na_lig
     fp = FFTProcess(0)
     fp.alloc_array(job.nf1, job.grid_width, job.grid_coord())
     rr, ri = job.receptor_grids()
@@ -79,7 +91,7 @@ def test_noalloc_matches_md_dock(built, gpu, pairs, name, extra):
 def test_noalloc_rejects_oversized_requests(built, gpu):
     from megadock_b200 import lib
     dummy = C.c_void_p(16)
-    # N = 160 needs more scratch than the fixed array holds
+    # N = 160 is above nf1 = 128, the largest edge the fixed scratch array is sized for
     rc = lib().md_dock_noalloc(160, C.c_float(1.2), dummy, dummy, 10, dummy, dummy, dummy, C.c_float(1.0), dummy,
                                0, 1, 1, dummy, None)
     assert rc == 4
