@@ -834,32 +834,46 @@ __global__ void __launch_bounds__(16 * LT, xline_occ<N>() / LT)
     for (int pass = 0; pass < passes; ++pass) {
         const int kyo = pass == 0 ? ky : NH;   // own row
         const int kym = (N - kyo) % N;         // mirror row
-        // forward x pass 1 on both tiles, straight from global (pruned rows)
-        for (int it = threadIdx.x; it < 2 * LT * R2; it += blockDim.x) {
+        // forward x pass 1 on both tiles, straight from global (pruned rows):
+        // every item of this thread issues its loads before the first DFT, so
+        // the HBM latency is paid once per thread, not once per item
+        constexpr int IT1 = (2 * LT * R2 + NT - 1) / NT;
+        float2 v1[IT1][R1];
+#pragma unroll
+        for (int r = 0; r < IT1; ++r) {
+            const int it = threadIdx.x + r * NT;
             const int s = it / (LT * R2);
             const int t = (it / LT) % R2;
             const int row = s ? kym : kyo, col = s ? kzm : kz;
-            float2 v[R1];
+            const bool live = ok && it < 2 * LT * R2;
             static_for<0, R1>([&](auto m_) {
                 constexpr int mm = decltype(m_)::value;
                 const int pp = t + R2 * mm - OFF;   // spectrum plane of x = t + R2 mm, if any
                 if constexpr (PR && (mm < R1 / 4 || mm >= 3 * R1 / 4)) {
-                    v[mm] = make_float2(0.f, 0.f);
+                    v1[r][mm] = make_float2(0.f, 0.f);
                 } else if constexpr (PR) {
-                    v[mm] = ok ? Ab[((size_t)pp * N + row) * N + col] : make_float2(0.f, 0.f);
+                    v1[r][mm] = live ? Ab[((size_t)pp * N + row) * N + col] : make_float2(0.f, 0.f);
                 } else {
-                    v[mm] = (ok && (unsigned)pp < (unsigned)NG) ? Ab[((size_t)pp * N + row) * N + col]
-                                                                : make_float2(0.f, 0.f);
+                    v1[r][mm] = (live && (unsigned)pp < (unsigned)NG) ? Ab[((size_t)pp * N + row) * N + col]
+                                                                     : make_float2(0.f, 0.f);
                 }
             });
-            Dft<R1, -1>::run(v);
-            float2 *X = s ? X1 : X0;
-            static_for<0, R1>([&](auto k1_) {
-                constexpr int k1 = decltype(k1_)::value;
-                float2 x = v[k1];
-                if constexpr (k1 != 0) x = cmul(x, __ldg(&G.tw[t * k1]));
-                X[(k1 * R2 + t) * LT + lane] = x;
-            });
+        }
+#pragma unroll
+        for (int r = 0; r < IT1; ++r) {
+            const int it = threadIdx.x + r * NT;
+            if (it < 2 * LT * R2) {
+                const int s = it / (LT * R2);
+                const int t = (it / LT) % R2;
+                Dft<R1, -1>::run(v1[r]);
+                float2 *X = s ? X1 : X0;
+                static_for<0, R1>([&](auto k1_) {
+                    constexpr int k1 = decltype(k1_)::value;
+                    float2 x = v1[r][k1];
+                    if constexpr (k1 != 0) x = cmul(x, __ldg(&G.tw[t * k1]));
+                    X[(k1 * R2 + t) * LT + lane] = x;
+                });
+            }
         }
         __syncthreads();
         // forward x pass 2 and the conj(R^) product, held in registers
