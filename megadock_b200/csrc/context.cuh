@@ -171,12 +171,9 @@ struct Sized {
             k_plane_fwd<N, MODE><<<dim3(NG, nb), kNT1, smem_fwd(), s>>>(L, G, vbits, qlist, qcount, sr, si, A, vr, vi);
     }
     template <int LT = kLT>
-    static size_t smem_xline() { return (size_t)2 * N * LT * sizeof(float2); }
+    static size_t smem_xline() { return xline_smem<N, LT>(); }
     template <int V = 0>
-    static size_t smem_c2r() {
-        constexpr int PA = N + C2RPlan<N, V>::R1, PB = N + 8;
-        return (size_t)NH * (PA > PB ? PA : PB) * sizeof(float2);
-    }
+    static size_t smem_c2r() { return c2r_smem<N, V>(); }
 
     static cudaError_t set_attrs() {
         static bool done = false;

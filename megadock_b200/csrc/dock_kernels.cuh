@@ -803,11 +803,31 @@ __global__ void __launch_bounds__(kNT)
 //
 // xline_occ: threads per SM the kernel is compiled for, in units of 16:
 // 1,280 where that register budget (51 per thread) holds the kernel without
-// spills, 512 above N = 160 (radices up to 20 need the registers), else 1,024.  B200, 13,824 rotations at 192 per launch: +2.0 % at
-// N=96; with spills at N=112 and 128 it lost 2 % and 7 %.
+// spills, 512 above N = 160 (radices up to 20 need the registers), else 1,024.
+// B200, 13,824 rotations at 192 per launch: +2.0 % at N=96; with spills at
+// N=112 it lost 2 %.  N = 128 runs 1,280 since its first-pass loads are issued
+// ahead of the DFTs and its twiddles come from shared memory (xline_tw_smem).
 template <int N>
 constexpr int xline_occ() {
-    return (N == 32 || N == 64 || N == 72 || N == 80 || N == 96) ? 80 : (N > 160 ? 32 : 64);
+    return (N == 32 || N == 64 || N == 72 || N == 80 || N == 96 || N == 128) ? 80 : (N > 160 ? 32 : 64);
+}
+
+// Twiddles of the x-line kernel from shared memory instead of the read-only
+// cache.  Measured at N = 128 (B200, 54,000 rotations, 192 per launch): with
+// five 256-thread CTAs per SM (48 registers) 267 ms per step for this kernel,
+// against 277 ms with cached loads and 278 ms at four CTAs per SM; at four
+// CTAs per SM the shared-memory table lost (285 ms).  Other sizes keep the
+// cached loads.
+template <int N>
+constexpr bool xline_tw_smem() {
+    return N == 128;
+}
+
+// Shared memory of k_xline_herm: the own and mirror tiles, and the twiddle
+// table where xline_tw_smem<N>().
+template <int N, int LT>
+constexpr size_t xline_smem() {
+    return (size_t)(2 * N * LT + (xline_tw_smem<N>() ? N : 0)) * sizeof(float2);
 }
 
 template <int N, int LT = kLT>
@@ -821,6 +841,15 @@ __global__ void __launch_bounds__(16 * LT, xline_occ<N>() / LT)
     float2 *X0 = reinterpret_cast<float2 *>(smem_raw);   // own tile   [N][LT]
     float2 *X1 = X0 + N * LT;                           // mirror tile [N][LT]
     constexpr int NT = 16 * LT;
+    float2 *TWs = X1 + N * LT;                          // twiddles W_N^j (xline_tw_smem)
+    if constexpr (xline_tw_smem<N>()) {
+        for (int e = threadIdx.x; e < N; e += NT) TWs[e] = __ldg(&G.tw[e]);
+        __syncthreads();
+    }
+    auto tw_at = [&](int j) {
+        if constexpr (xline_tw_smem<N>()) return TWs[j];
+        else return __ldg(&G.tw[j]);
+    };
     const int lane = threadIdx.x % LT;
     const int ky = blockIdx.x / TILES;
     const int kz = (blockIdx.x % TILES) * LT + lane;
@@ -870,7 +899,7 @@ __global__ void __launch_bounds__(16 * LT, xline_occ<N>() / LT)
                 static_for<0, R1>([&](auto k1_) {
                     constexpr int k1 = decltype(k1_)::value;
                     float2 x = v1[r][k1];
-                    if constexpr (k1 != 0) x = cmul(x, __ldg(&G.tw[t * k1]));
+                    if constexpr (k1 != 0) x = cmul(x, tw_at(t * k1));
                     X[(k1 * R2 + t) * LT + lane] = x;
                 });
             }
@@ -921,7 +950,7 @@ __global__ void __launch_bounds__(16 * LT, xline_occ<N>() / LT)
             static_for<0, R1>([&](auto k1_) {
                 constexpr int k1 = decltype(k1_)::value;
                 float2 x = v[k1];
-                if constexpr (k1 != 0) x = cmul(x, conjf2(__ldg(&G.tw[t * k1])));
+                if constexpr (k1 != 0) x = cmul(x, conjf2(tw_at(t * k1)));
                 X0[(k1 * R2 + t) * LT + lane] = x;
             });
         }
@@ -1065,6 +1094,13 @@ struct C2RPlan {
     static constexpr int Q2 = V == 2 ? Plan<N / 2>::R1 : Plan<N / 2>::R2;
 };
 
+// Shared memory of k_plane_c2r: the N/2 x PITCH plane.
+template <int N, int V>
+constexpr size_t c2r_smem() {
+    constexpr size_t PA = N + C2RPlan<N, V>::R1, PB = N + 8;
+    return (size_t)(N / 2) * (PA > PB ? PA : PB) * sizeof(float2);
+}
+
 template <int N, int T, int V = 0>
 constexpr int c2r_min_blocks() {
     using P = C2RPlan<N, V>;
@@ -1072,6 +1108,14 @@ constexpr int c2r_min_blocks() {
     if ((size_t)(N / 2) * pitch * 8 > 113 * 1024) return 1;   // one CTA per SM by shared memory
     return (T <= 4 && P::R1 <= 8 && P::R2 <= 16 && P::Q1 <= 8 && P::Q2 <= 16) ? 3 : 2;
 }
+
+// The plane kernel's item loops: items tid, tid + kNT, ... below COUNT, with
+// a compile-time trip count (blockDim.x is always kNT here) so that each loop
+// unrolls (3.4 % less time for this kernel at N = 128 than the runtime-bounded
+// loops).
+#define MDB_K3_ITEMS(it, COUNT)                                                                 \
+    _Pragma("unroll") for (int r_##it = 0; r_##it < ((COUNT) + kNT - 1) / kNT; ++r_##it)       \
+        if (const int it = tid + r_##it * kNT; ((COUNT) % kNT == 0) || it < (COUNT))
 
 template <int N, int T, int V = 0>
 __global__ void __launch_bounds__(kNT, c2r_min_blocks<N, T, V>())
@@ -1085,13 +1129,14 @@ __global__ void __launch_bounds__(kNT, c2r_min_blocks<N, T, V>())
     constexpr int PITCH = PA > PB ? PA : PB;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     float2 *S = reinterpret_cast<float2 *>(smem_raw);   // NH x PITCH
+    auto tw_at = [&](int j) { return __ldg(&G.tw[j]); };
     const int x = blockIdx.x;
     const int b = blockIdx.y;
     const int tid = threadIdx.x;
     const float2 *Gp = Gh + ((size_t)b * N + x) * NH * N;
 
     // (1a) inverse kz pass 1, straight from global: item = (row, t), t fastest
-    for (int it = tid; it < NH * R2; it += blockDim.x) {
+    MDB_K3_ITEMS(it, NH * R2) {
         const int row = it / R2, t = it % R2;
         float2 v[R1];
         static_for<0, R1>([&](auto m_) {
@@ -1102,7 +1147,7 @@ __global__ void __launch_bounds__(kNT, c2r_min_blocks<N, T, V>())
         static_for<0, R1>([&](auto k1_) {
             constexpr int k1 = decltype(k1_)::value;
             float2 xv = v[k1];
-            if constexpr (k1 != 0) xv = cmul(xv, conjf2(__ldg(&G.tw[t * k1])));
+            if constexpr (k1 != 0) xv = cmul(xv, conjf2(tw_at(t * k1)));
             S[row * PITCH + k1 * (R2 + 1) + t] = xv;
         });
     }
@@ -1135,7 +1180,7 @@ __global__ void __launch_bounds__(kNT, c2r_min_blocks<N, T, V>())
     }
     __syncthreads();
     // (2a) fold the half spectrum into Z, in place (pairs k, N/2-k)
-    for (int it = tid; it < N * (NH / 2 + 1); it += blockDim.x) {
+    MDB_K3_ITEMS(it, N * (NH / 2 + 1)) {
         const int z = it % N, k = it / N;
         if (k == 0) {
             const float2 v = S[z];   // X0 + i X_{N/2}, both real
@@ -1143,7 +1188,7 @@ __global__ void __launch_bounds__(kNT, c2r_min_blocks<N, T, V>())
         } else {
             const int k2 = NH - k;
             const float2 a = S[k * PITCH + z], c = S[k2 * PITCH + z];
-            const float2 wk = conjf2(__ldg(&G.tw[k])), wk2 = conjf2(__ldg(&G.tw[k2]));
+            const float2 wk = conjf2(tw_at(k)), wk2 = conjf2(tw_at(k2));
             // E = a + conj(c), D = a - conj(c), Z = E + i w^k D
             const float2 e1 = make_float2(a.x + c.x, a.y - c.y), d1 = make_float2(a.x - c.x, a.y + c.y);
             const float2 o1 = cmul(wk, d1);
@@ -1158,7 +1203,7 @@ __global__ void __launch_bounds__(kNT, c2r_min_blocks<N, T, V>())
     }
     __syncthreads();
     // (2b) N/2-point inverse along ky, pass 1 (lanes = z), in place
-    for (int it = tid; it < N * Q2; it += blockDim.x) {
+    MDB_K3_ITEMS(it, N * Q2) {
         const int z = it % N, tt = it / N;
         float2 v[Q1];
         static_for<0, Q1>([&](auto m_) {
@@ -1169,7 +1214,7 @@ __global__ void __launch_bounds__(kNT, c2r_min_blocks<N, T, V>())
         static_for<0, Q1>([&](auto k1_) {
             constexpr int k1 = decltype(k1_)::value;
             float2 xv = v[k1];
-            if constexpr (k1 != 0) xv = cmul(xv, conjf2(__ldg(&G.tw[2 * tt * k1])));
+            if constexpr (k1 != 0) xv = cmul(xv, conjf2(tw_at(2 * tt * k1)));
             S[(k1 * Q2 + tt) * PITCH + z] = xv;
         });
     }
@@ -1215,7 +1260,7 @@ __global__ void __launch_bounds__(kNT, c2r_min_blocks<N, T, V>())
         // (2c) pass 2 in place: every item writes its scores back over the
         // slots it read and keeps its thread's largest score.
         float tmax = -INFINITY;   // fmaxf drops NaN keys, which are never selected
-        for (int it = tid; it < N * Q1; it += blockDim.x) {
+        MDB_K3_ITEMS(it, N * Q1) {
             const int z = it % N, u = it / N;
             float2 o[Q2];
             static_for<0, Q2>([&](auto n2_) {
@@ -1255,7 +1300,7 @@ __global__ void __launch_bounds__(kNT, c2r_min_blocks<N, T, V>())
         // the few threads holding a score at or above the bound insert theirs
         // (each thread reads back only the slots it wrote)
         if (tmax >= thr) {
-            for (int it = tid; it < N * Q1; it += blockDim.x) {
+            MDB_K3_ITEMS(it, N * Q1) {
                 const int z = it % N, u = it / N;
                 const int cell0 = base + 2 * u * N + z;
                 static_for<0, Q2>([&](auto k2_) {

@@ -78,11 +78,8 @@ int tw_offset(int n) {
 template <int N>
 struct Smem {
     static size_t fwd() { return (size_t)N * (N + 1) * sizeof(float2); }
-    static size_t xline() { return (size_t)2 * N * kLT * sizeof(float2); }
-    static size_t c2r() {
-        constexpr int PA = N + Plan<N>::R1, PB = N + 8;
-        return (size_t)(N / 2) * (PA > PB ? PA : PB) * sizeof(float2);
-    }
+    static size_t xline() { return xline_smem<N, kLT>(); }
+    static size_t c2r() { return c2r_smem<N, 0>(); }
 };
 
 template <int N>
