@@ -128,7 +128,8 @@ int md_dock_profile(md_ctx *ctx, const float *d_rotmat, int first_rot, int n_rot
  * device: the rPSC/ACE real grid and the electrostatic grid of na receptor
  * atoms (coordinates centred on the receptor, radius, charge and ACE value
  * per atom; -a, -d and -e values), bit-exact with the reference's CPU code
- * for grids up to ng1 = 112.  make_receptor = 1 also makes them this
+ * for grids up to ng1 = 256 (every size the docking kernels are built for).
+ * make_receptor = 1 also makes them this
  * context's receptor (R^ for md_dock, and the grids for the adjoint), as
  * md_receptor_fft would; grid_r / grid_i (ng1^3 host floats, may be NULL)
  * receive a copy.  Needs md_set_grid. */

@@ -18,16 +18,23 @@
 
 #include "../../include/md_b200.h"
 #include "dock_kernels.cuh"
+#include "staged_kernels.cuh"
 
 using namespace mdb;
 
 namespace mdb {
 
+// Candidate groups per rotation from the top-t kernels: one per x-plane, or
+// one per (x-plane, column block) for the staged sizes.
+inline size_t cand_groups(size_t N) {
+    return N > (size_t)kMaxResidentN ? N * ((N + kCB - 1) / kCB) : N;
+}
+
 // Per-launch intermediates for `cap` rotations of one launch group.
 struct WorkSet {
     float2 *A = nullptr;        // [cap][N/2][N][N]    spectrum planes (K1 -> K2)
     float2 *G = nullptr;        // [cap][N][N/2][N]    Hermitian half (K2 -> K3)
-    Cand *cand = nullptr;       // [cap][N][t]         per-plane candidates (K3 -> K4)
+    Cand *cand = nullptr;       // [cap][groups][t]    per-plane candidates (K3 -> K4)
     uint32_t *vbits = nullptr;  // [cap][N/2][2][N/2 * words per row] voxel classes (K0 -> K1)
     int2 *qlist = nullptr;      // [cap][N/2][(N/2)^2] charged cells per voxel plane (K0 -> K1)
     int *qcount = nullptr;      // [cap][N/2]
@@ -59,7 +66,7 @@ struct WorkSet {
     static Sizes need(size_t cap, size_t N, size_t t, size_t na) {
         const size_t NG = N / 2;
         return Sizes{{sizeof(float2) * cap * NG * N * N, sizeof(float2) * cap * N * (N / 2) * N,
-                      sizeof(Cand) * cap * N * t, sizeof(uint32_t) * cap * NG * 2 * NG * ((NG + 31) / 32),
+                      sizeof(Cand) * cap * cand_groups(N) * t, sizeof(uint32_t) * cap * NG * 2 * NG * ((NG + 31) / 32),
                       sizeof(int2) * cap * NG * NG * NG, sizeof(int) * cap * NG, sizeof(MarkEntry) * cap * na,
                       sizeof(int) * cap * (NG + 2 * kReach + 1), sizeof(int2) * cap * na, sizeof(int) * cap * (NG + 1),
                       sizeof(uint32_t) * cap * NG * 2 * NG * ((NG + 31) / 32)}};
@@ -146,6 +153,10 @@ struct Sized {
     static constexpr int NG = N / 2;
     static constexpr int NH = N / 2;
     static constexpr int TILES = (N + kLT - 1) / kLT;
+    // above 224 the plane transforms run as row and column launches
+    // (staged_kernels.cuh)
+    static constexpr bool kStaged = staged<N>();
+    static constexpr int ZB = c2r_zblocks<N>();
     static size_t smem_fwd() { return (size_t)N * (N + 1) * sizeof(float2); }
     static size_t smem_xrec() { return (size_t)N * kLT * sizeof(float2); }
     static size_t smem_vox() { return vox_bits_smem<NG>(); }
@@ -182,30 +193,59 @@ struct Sized {
         auto set = [&](const void *f, size_t bytes) {
             if (e == cudaSuccess) e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
         };
-        set_fwd<0>(set);
-        set_fwd<1>(set);
-        set_fwd<2>(set);
+        if constexpr (kStaged) {
+            set((const void *)k_rows_fwd<N, 0>, rows_smem(N));
+            set((const void *)k_rows_fwd<N, 1>, rows_smem(N));
+            set((const void *)k_rows_fwd<N, 2>, rows_smem(N));
+            set((const void *)k_cols_fwd<N>, cols_fwd_smem(N));
+            set((const void *)k_rows_inv<N>, rows_smem(N));
+            set((const void *)k_cols_c2r<N, 1>, cols_c2r_smem(N));
+            set((const void *)k_cols_c2r<N, 4>, cols_c2r_smem(N));
+            set((const void *)k_cols_c2r<N, 16>, cols_c2r_smem(N));
+        } else {
+            set_fwd<0>(set);
+            set_fwd<1>(set);
+            set_fwd<2>(set);
+            set((const void *)k_plane_c2r<N, 1, 0>, smem_c2r<0>());
+            set((const void *)k_plane_c2r<N, 4, 0>, smem_c2r<0>());
+            set((const void *)k_plane_c2r<N, 16, 0>, smem_c2r<0>());
+            set((const void *)k_plane_c2r<N, 1, 1>, smem_c2r<1>());
+            set((const void *)k_plane_c2r<N, 4, 1>, smem_c2r<1>());
+            set((const void *)k_plane_c2r<N, 1, 2>, smem_c2r<2>());
+            set((const void *)k_plane_c2r<N, 4, 2>, smem_c2r<2>());
+        }
         set((const void *)k_xline_rec<N>, smem_xrec());
         set((const void *)k_vox_bits<NG, true>, smem_vox());
         set((const void *)k_vox_bits<NG, false>, smem_vox());
         set((const void *)k_xline_herm<N, 32>, smem_xline<32>());
         set((const void *)k_xline_herm<N, 16>, smem_xline<16>());
         set((const void *)k_xline_herm<N, 8>, smem_xline<8>());
-        set((const void *)k_plane_c2r<N, 1, 0>, smem_c2r<0>());
-        set((const void *)k_plane_c2r<N, 4, 0>, smem_c2r<0>());
-        set((const void *)k_plane_c2r<N, 16, 0>, smem_c2r<0>());
-        set((const void *)k_plane_c2r<N, 1, 1>, smem_c2r<1>());
-        set((const void *)k_plane_c2r<N, 4, 1>, smem_c2r<1>());
-        set((const void *)k_plane_c2r<N, 1, 2>, smem_c2r<2>());
-        set((const void *)k_plane_c2r<N, 4, 2>, smem_c2r<2>());
         if (e == cudaSuccess) done = true;
         return e;
+    }
+
+    // Forward plane transforms of nb rotations (MODE 0/1) or the voxel planes
+    // themselves (MODE 2) in the staged form: row launch, then column launch.
+    template <int MODE>
+    static void staged_fwd(cudaStream_t s, int nb, const LigandView &L, const GridView &G, const uint32_t *vbits,
+                           const int2 *qlist, const int *qcount, const float *sr, const float *si, float2 *A,
+                           float *vr, float *vi) {
+        k_rows_fwd<N, MODE><<<dim3(NG, (NG + kRB - 1) / kRB, nb), kNTS, rows_smem(N), s>>>(L, G, vbits, qlist, qcount,
+                                                                                           sr, si, A, vr, vi);
+        if constexpr (MODE != 2) k_cols_fwd<N><<<dim3(NG, (N + kCB - 1) / kCB, nb), kNTS, cols_fwd_smem(N), s>>>(G, A);
+    }
+    template <int MODE>
+    static void any_fwd(cudaStream_t s, int nb, const LigandView &L, const GridView &G, const uint32_t *vbits,
+                        const int2 *qlist, const int *qcount, const float *sr, const float *si, float2 *A, float *vr,
+                        float *vi) {
+        if constexpr (kStaged) staged_fwd<MODE>(s, nb, L, G, vbits, qlist, qcount, sr, si, A, vr, vi);
+        else plane_fwd<MODE>(s, nb, L, G, vbits, qlist, qcount, sr, si, A, vr, vi);
     }
 
     static void receptor(md_ctx *c, const float *d_r, const float *d_i) {
         GridView G{c->ng, c->gw, 0.f, c->d_gc, c->d_tw};
         LigandView L{0, nullptr, nullptr, 1.f};
-        plane_fwd<1>(c->stream, 1, L, G, nullptr, nullptr, nullptr, d_r, d_i, c->ws[0].A, nullptr, nullptr);
+        any_fwd<1>(c->stream, 1, L, G, nullptr, nullptr, nullptr, d_r, d_i, c->ws[0].A, nullptr, nullptr);
         k_xline_rec<N><<<dim3(N * TILES, 1), kNT, smem_xrec(), c->stream>>>(G, c->ws[0].A, c->d_Rh);
     }
 
@@ -225,7 +265,7 @@ struct Sized {
         LigandView L{c->na, c->d_atom, c->d_rad2, c->delta};
         const WorkSet &w = c->ws[0];
         voxelize(c, w, d_rot9, nb, c->stream);
-        plane_fwd<2>(c->stream, nb, L, G, w.vbits, w.qlist, w.qcount, nullptr, nullptr, nullptr, d_vr, d_vi);
+        any_fwd<2>(c->stream, nb, L, G, w.vbits, w.qlist, w.qcount, nullptr, nullptr, nullptr, d_vr, d_vi);
     }
 
     static void voxels(md_ctx *c, const float *d_rot9, float *d_vr, float *d_vi) {
@@ -233,7 +273,7 @@ struct Sized {
         LigandView L{c->na, c->d_atom, c->d_rad2, c->delta};
         const WorkSet &w = c->ws[0];
         voxelize(c, w, d_rot9, 1, c->stream);
-        plane_fwd<2>(c->stream, 1, L, G, w.vbits, w.qlist, w.qcount, nullptr, nullptr, nullptr, d_vr, d_vi);
+        any_fwd<2>(c->stream, 1, L, G, w.vbits, w.qlist, w.qcount, nullptr, nullptr, nullptr, d_vr, d_vi);
     }
 
     // The plane top-t kernel in passes of T candidates (T = 1, 4 or 16), with
@@ -243,21 +283,32 @@ struct Sized {
                     int nsel, Cand *cand) {
         k_plane_c2r<N, T, V><<<dim3(N, nb), kNT, smem_c2r<V>(), s>>>(G, Gh, t, nf3f, out0, nsel, cand);
     }
-    static void plane_topt(cudaStream_t s, const GridView &G, const float2 *Gh, int nb, int t, float nf3f, Cand *cand,
+    static void plane_topt(cudaStream_t s, const GridView &G, float2 *Gh, int nb, int t, float nf3f, Cand *cand,
                            int plan) {
         const int T = t == 1 ? 1 : (t <= 4 ? 4 : 16);
-        for (int out0 = 0; out0 < t; out0 += T) {
-            const int nsel = std::min(T, t - out0);
-            if (T == 1) {
-                if (plan == 1) c2r<1, 1>(s, G, Gh, nb, t, nf3f, out0, nsel, cand);
-                else if (plan == 2) c2r<1, 2>(s, G, Gh, nb, t, nf3f, out0, nsel, cand);
-                else c2r<1, 0>(s, G, Gh, nb, t, nf3f, out0, nsel, cand);
-            } else if (T == 4) {
-                if (plan == 1) c2r<4, 1>(s, G, Gh, nb, t, nf3f, out0, nsel, cand);
-                else if (plan == 2) c2r<4, 2>(s, G, Gh, nb, t, nf3f, out0, nsel, cand);
-                else c2r<4, 0>(s, G, Gh, nb, t, nf3f, out0, nsel, cand);
-            } else {
-                c2r<16, 0>(s, G, Gh, nb, t, nf3f, out0, nsel, cand);
+        if constexpr (kStaged) {
+            k_rows_inv<N><<<dim3(N, (NH + kRB - 1) / kRB, nb), kNTS, rows_smem(N), s>>>(G, Gh);
+            for (int out0 = 0; out0 < t; out0 += T) {
+                const int nsel = std::min(T, t - out0);
+                const dim3 grid(N, ZB, nb);
+                if (T == 1) k_cols_c2r<N, 1><<<grid, kNTS, cols_c2r_smem(N), s>>>(G, Gh, t, out0, nsel, cand);
+                else if (T == 4) k_cols_c2r<N, 4><<<grid, kNTS, cols_c2r_smem(N), s>>>(G, Gh, t, out0, nsel, cand);
+                else k_cols_c2r<N, 16><<<grid, kNTS, cols_c2r_smem(N), s>>>(G, Gh, t, out0, nsel, cand);
+            }
+        } else {
+            for (int out0 = 0; out0 < t; out0 += T) {
+                const int nsel = std::min(T, t - out0);
+                if (T == 1) {
+                    if (plan == 1) c2r<1, 1>(s, G, Gh, nb, t, nf3f, out0, nsel, cand);
+                    else if (plan == 2) c2r<1, 2>(s, G, Gh, nb, t, nf3f, out0, nsel, cand);
+                    else c2r<1, 0>(s, G, Gh, nb, t, nf3f, out0, nsel, cand);
+                } else if (T == 4) {
+                    if (plan == 1) c2r<4, 1>(s, G, Gh, nb, t, nf3f, out0, nsel, cand);
+                    else if (plan == 2) c2r<4, 2>(s, G, Gh, nb, t, nf3f, out0, nsel, cand);
+                    else c2r<4, 0>(s, G, Gh, nb, t, nf3f, out0, nsel, cand);
+                } else {
+                    c2r<16, 0>(s, G, Gh, nb, t, nf3f, out0, nsel, cand);
+                }
             }
         }
     }
@@ -272,7 +323,7 @@ struct Sized {
         const float nf3f = (float)((long long)N * N * N);
         voxelize(c, w, d_rot9, nb, s);
         if (ev) cudaEventRecord(ev[1], s);
-        plane_fwd<0>(s, nb, L, G, w.vbits, w.qlist, w.qcount, nullptr, nullptr, w.A, nullptr, nullptr);
+        any_fwd<0>(s, nb, L, G, w.vbits, w.qlist, w.qcount, nullptr, nullptr, w.A, nullptr, nullptr);
         if (ev) cudaEventRecord(ev[2], s);
         if (c->tile == 16)
             k_xline_herm<N, 16><<<dim3(NH * ((N + 15) / 16), nb), 256, smem_xline<16>(), s>>>(G, w.A, c->d_Rh, w.G);
@@ -283,7 +334,7 @@ struct Sized {
         if (ev) cudaEventRecord(ev[3], s);
         plane_topt(s, G, w.G, nb, t, nf3f, w.cand, c->plan);
         if (ev) cudaEventRecord(ev[4], s);
-        k_merge<<<nb, 256, 0, s>>>(w.cand, N, t, N, nf3f, rot0, d_pose);
+        k_merge<<<nb, 256, 0, s>>>(w.cand, kStaged ? N * ZB : N, t, N, nf3f, rot0, d_pose);
         if (ev) cudaEventRecord(ev[5], s);
     }
 };
@@ -320,6 +371,9 @@ const SizedOps *sized_ops_g(int N);
 const SizedOps *sized_ops_h(int N);
 const SizedOps *sized_ops_i(int N);
 const SizedOps *sized_ops_j(int N);
+const SizedOps *sized_ops_k(int N);
+const SizedOps *sized_ops_l(int N);
+const SizedOps *sized_ops_m(int N);
 
 inline const SizedOps *sized_ops(int N) {
     if (const SizedOps *o = sized_ops_a(N)) return o;
@@ -331,7 +385,10 @@ inline const SizedOps *sized_ops(int N) {
     if (const SizedOps *o = sized_ops_g(N)) return o;
     if (const SizedOps *o = sized_ops_h(N)) return o;
     if (const SizedOps *o = sized_ops_i(N)) return o;
-    return sized_ops_j(N);
+    if (const SizedOps *o = sized_ops_j(N)) return o;
+    if (const SizedOps *o = sized_ops_k(N)) return o;
+    if (const SizedOps *o = sized_ops_l(N)) return o;
+    return sized_ops_m(N);
 }
 
 }  // namespace mdb

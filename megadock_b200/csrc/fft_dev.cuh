@@ -295,6 +295,25 @@ MDB_PLAN(210, 14, 15)
 MDB_PLAN(216, 12, 18)
 MDB_PLAN(220, 20, 11)
 MDB_PLAN(224, 16, 14)
+// half edges of the staged sizes' complex-to-real pass
+MDB_PLAN(121, 11, 11)
+MDB_PLAN(125, 5, 25)
+MDB_PLAN(135, 5, 27)
+MDB_PLAN(147, 7, 21)
+// edges above 224 (ng1 of the default grid table up to 160): staged kernels
+MDB_PLAN(240, 16, 15)
+MDB_PLAN(242, 22, 11)
+MDB_PLAN(250, 10, 25)
+MDB_PLAN(252, 12, 21)
+MDB_PLAN(256, 16, 16)
+MDB_PLAN(264, 12, 22)
+MDB_PLAN(270, 10, 27)
+MDB_PLAN(280, 20, 14)
+MDB_PLAN(288, 16, 18)
+MDB_PLAN(294, 14, 21)
+MDB_PLAN(300, 20, 15)
+MDB_PLAN(308, 28, 11)
+MDB_PLAN(320, 16, 20)
 #undef MDB_PLAN
 
 // Whether the first passes of an axis of length N can skip the zero padding

@@ -245,7 +245,7 @@ int md_set_grid(md_ctx *ctx, int nf1, float grid_width, const float *grid_coord)
     if (!ctx || !grid_coord || !(grid_width > 0.f)) return MD_ERR_ARG;
     if (!size_supported(nf1)) {
         ctx->err = "FFT size " + std::to_string(nf1) +
-                   " has no built kernel set (built: the grid-table sizes up to 224; -F picks one)";
+                   " has no built kernel set (built: the default grid table's sizes up to 320; -F picks one)";
         return MD_ERR_SIZE;
     }
     MD_CUDA(cudaSetDevice(ctx->device));
@@ -344,6 +344,7 @@ int md_receptor_build(md_ctx *ctx, int na, const float *xyz_centred, const float
     float *d_xyz = nullptr, *d_rad = nullptr, *d_q = nullptr, *d_ace = nullptr, *d_grid = nullptr;
     RecAtom *d_atoms = nullptr;
     int *d_cnt = nullptr, *d_start = nullptr, *d_list = nullptr;
+    void *d_masks = nullptr;   // sweep row masks above ng = kRecSmemNg
     cudaError_t e = cudaSuccess;
     auto step = [&](cudaError_t x) {
         if (e == cudaSuccess) e = x;
@@ -357,6 +358,7 @@ int md_receptor_build(md_ctx *ctx, int na, const float *xyz_centred, const float
         cudaFree(d_cnt);
         cudaFree(d_start);
         cudaFree(d_list);
+        cudaFree(d_masks);
         if (!make_receptor) cudaFree(d_grid);
     };
     cudaStream_t s = ctx->stream;
@@ -381,9 +383,25 @@ int md_receptor_build(md_ctx *ctx, int na, const float *xyz_centred, const float
     step(cudaMemcpyAsync(d_ace, ace, sizeof(float) * na, cudaMemcpyHostToDevice, s));
     step(cudaMemsetAsync(d_r, 0, sizeof(float) * ng3, s));
     const int rows = ng * ng;
-    const size_t sweep_smem = sizeof(RowMask) * rows;
-    step(cudaFuncSetAttribute(k_rec_sweep, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)(sizeof(RowMask) * kRecMaxNg * kRecMaxNg)));
+    // the two propagation sweeps: row masks of ceil(ng / 64) words, in shared
+    // memory up to ng = kRecSmemNg, else in a global buffer
+    auto sweep = [&]() {
+        if (ng <= kRecSmemNg) {
+            const size_t smem = sizeof(RowMask<2>) * rows;
+            step(cudaFuncSetAttribute(k_rec_sweep<2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)(sizeof(RowMask<2>) * kRecSmemNg * kRecSmemNg)));
+            for (int k = 0; k < 2 && e == cudaSuccess; ++k)
+                k_rec_sweep<2, false><<<1, 1024, smem, s>>>(P, d_r, open_space, nullptr);
+        } else if (ng <= 192) {
+            step(cudaMalloc(&d_masks, sizeof(RowMask<3>) * rows));
+            for (int k = 0; k < 2 && e == cudaSuccess; ++k)
+                k_rec_sweep<3, true><<<1, 1024, 0, s>>>(P, d_r, open_space, static_cast<RowMask<3> *>(d_masks));
+        } else {
+            step(cudaMalloc(&d_masks, sizeof(RowMask<4>) * rows));
+            for (int k = 0; k < 2 && e == cudaSuccess; ++k)
+                k_rec_sweep<4, true><<<1, 1024, 0, s>>>(P, d_r, open_space, static_cast<RowMask<4> *>(d_masks));
+        }
+    };
     const int cells_blocks = (int)((ng3 + 255) / 256);
     std::vector<int> cnt(rows + 1), start(rows + 1);
     auto scan = [&](int n) {   // counts -> starts on the host (n + 1 entries)
@@ -398,7 +416,7 @@ int md_receptor_build(md_ctx *ctx, int na, const float *xyz_centred, const float
         k_rec_prep<<<(na + 255) / 256, 256, 0, s>>>(P, d_xyz, d_rad, d_q, d_ace, d_atoms);
         k_rec_core<<<na, 128, 0, s>>>(P, d_atoms, ctx->d_gc, d_r);
         k_rec_rays<<<(3 * rows + 255) / 256, 256, 0, s>>>(P, d_r, open_space);
-        for (int sweep = 0; sweep < 2; ++sweep) k_rec_sweep<<<1, 1024, sweep_smem, s>>>(P, d_r, open_space);
+        sweep();
         k_rec_final<<<cells_blocks, 256, 0, s>>>(P, d_r, open_space);
         // surface shell over per-row atom lists
         k_rec_rows<<<(rows + 3) / 4, 128, 0, s>>>(P, d_atoms, ctx->d_gc, d_cnt, nullptr, nullptr);

@@ -31,7 +31,11 @@
 
 namespace mdb {
 
-constexpr int kRecMaxNg = 112;   // row masks are two 64-bit words; 16 B x 112^2 of shared memory
+// Row masks of the propagation sweep: ceil(ng / 64) 64-bit words per (i, j)
+// row.  Up to ng = 112 every row's mask fits one CTA's shared memory (two
+// words, 16 B x 112^2); larger grids keep them in a global scratch buffer.
+constexpr int kRecSmemNg = 112;
+constexpr int kRecMaxNg = 256;
 
 struct RecAtom {
     float x, y, z;
@@ -131,15 +135,23 @@ __global__ void k_rec_rays(RecParams P, float *__restrict__ grid, float open_spa
     }
 }
 
+template <int WORDS>
 struct RowMask {
-    unsigned long long w[2];
+    unsigned long long w[WORDS];
 };
 
-__device__ __forceinline__ bool mbit(const RowMask &m, int k) { return (m.w[k >> 6] >> (k & 63)) & 1ull; }
+template <int WORDS>
+__device__ __forceinline__ bool mbit(const RowMask<WORDS> &m, int k) {
+    return (m.w[k >> 6] >> (k & 63)) & 1ull;
+}
 
-// One propagation sweep; one CTA.  smem: R masks of every row (ng^2 RowMask).
-__global__ void __launch_bounds__(1024) k_rec_sweep(RecParams P, float *__restrict__ grid, float open_space) {
-    extern __shared__ RowMask Rm[];
+// One propagation sweep; one CTA.  The R masks of every row (ng^2 of them)
+// live in dynamic shared memory, or with GMEM in `gmask` (ng^2 entries).
+template <int WORDS, bool GMEM>
+__global__ void __launch_bounds__(1024)
+    k_rec_sweep(RecParams P, float *__restrict__ grid, float open_space, RowMask<WORDS> *__restrict__ gmask) {
+    extern __shared__ __align__(16) unsigned char rec_smem[];
+    RowMask<WORDS> *Rm = GMEM ? gmask : reinterpret_cast<RowMask<WORDS> *>(rec_smem);
     const int ng = P.ng;
     const size_t ng2 = (size_t)ng * ng;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
@@ -149,7 +161,7 @@ __global__ void __launch_bounds__(1024) k_rec_sweep(RecParams P, float *__restri
         for (int i = ilo + warp; i <= ihi; i += nwarps) {
             const int j = d - i;
             const float *row = grid + (size_t)i * ng2 + (size_t)j * ng;
-            RowMask O{{0, 0}}, Z{{0, 0}};
+            RowMask<WORDS> O{}, Z{};
             for (int k0 = 0; k0 < ng; k0 += 32) {
                 const int k = k0 + lane;
                 const float v = k < ng ? row[k] : 1.0f;
@@ -159,22 +171,22 @@ __global__ void __launch_bounds__(1024) k_rec_sweep(RecParams P, float *__restri
                 Z.w[k0 >> 6] |= (unsigned long long)z << (k0 & 63);
             }
             if (lane == 0) {
-                RowMask In{{0, 0}};
+                RowMask<WORDS> In{};
                 if (j > 0 && vrow(i, j - 1)) {
-                    const RowMask &q = Rm[(size_t)i * ng + j - 1];
-                    In.w[0] |= q.w[0];
-                    In.w[1] |= q.w[1];
+                    const RowMask<WORDS> q = Rm[(size_t)i * ng + j - 1];
+#pragma unroll
+                    for (int w = 0; w < WORDS; ++w) In.w[w] |= q.w[w];
                 }
                 if (i > 0 && vrow(i - 1, j)) {
-                    const RowMask &q = Rm[(size_t)(i - 1) * ng + j];
-                    In.w[0] |= q.w[0];
-                    In.w[1] |= q.w[1];
+                    const RowMask<WORDS> q = Rm[(size_t)(i - 1) * ng + j];
+#pragma unroll
+                    for (int w = 0; w < WORDS; ++w) In.w[w] |= q.w[w];
                 }
                 const bool vr = vrow(i, j);
                 // Vk: positions 2 <= k <= ng - 2 (as a source on the k axis)
-                RowMask Vk{{0, 0}};
+                RowMask<WORDS> Vk{};
 #pragma unroll
-                for (int w = 0; w < 2; ++w) {
+                for (int w = 0; w < WORDS; ++w) {
                     const int lo = max(2 - 64 * w, 0), hi = min(ng - 2 - 64 * w, 63);   // bit range in word w
                     if (hi >= lo)
                         Vk.w[w] = ((hi - lo == 63) ? ~0ull : ((1ull << (hi - lo + 1)) - 1ull)) << lo;
@@ -184,11 +196,13 @@ __global__ void __launch_bounds__(1024) k_rec_sweep(RecParams P, float *__restri
                 // carry chain: within a run of P, everything from the first
                 // position after a reached cell up to the run's end is reached,
                 // i.e. P & (~(P + B) | B) with B = (R << 1) & P restricted to
-                // the seeds (the addition carries through the run).
-                RowMask R{{0, 0}};
+                // the seeds (the addition carries through the run); a run
+                // crossing a word boundary takes the previous word's top bit
+                // of R as its carry in.
+                RowMask<WORDS> R{};
                 unsigned long long carry = 0ull;   // R at bit 63 of the previous word
 #pragma unroll
-                for (int w = 0; w < 2; ++w) {
+                for (int w = 0; w < WORDS; ++w) {
                     const unsigned long long S = O.w[w] | (Z.w[w] & In.w[w] & Vk.w[w]);
                     const unsigned long long vprev = (Vk.w[w] << 1) | (w ? (Vk.w[w - 1] >> 63) : 0ull);
                     const unsigned long long P = vr ? (Z.w[w] & vprev) : 0ull;
@@ -206,7 +220,7 @@ __global__ void __launch_bounds__(1024) k_rec_sweep(RecParams P, float *__restri
     // apply: forward-reached cells, then zero cells with a valid reached successor
     for (size_t c = threadIdx.x; c < ng2 * ng; c += blockDim.x) {
         const int i = (int)(c / ng2), j = (int)((c / ng) % ng), k = (int)(c % ng);
-        const RowMask &r = Rm[(size_t)i * ng + j];
+        const RowMask<WORDS> &r = Rm[(size_t)i * ng + j];
         if (mbit(r, k)) continue;   // written below, after every read of this sweep
         if (grid[c] != 0.0f) continue;
         bool b = false;

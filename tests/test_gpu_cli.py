@@ -64,3 +64,29 @@ def test_cli_matches_reference_out(built, gpu, pairs, tmp_path):
     for n in range(1, len(b) - 1):
         if gaps[n - 1] > 0.05 and gaps[n] > 0.05:
             assert tuple(np.round(b[n, :6], 6)) in ours_set, b[n]
+
+
+@needs_ref
+def test_cli_automatic_size_above_224(built, gpu, pairs, tmp_path):
+    """Automatic grid sizing that lands above FFT edge 224 (the 500/250-residue
+    pair at grid width 0.55 A needs ng1 = 120, N = 240): the device receptor
+    build and the staged kernels give the reference's .out."""
+    from megadock_b200 import _native
+    from oracle.ref import REF_BIN
+    rp, lp = pairs["c1"]
+    flags = ["-R", rp, "-L", lp, "-v", "0.55", "-r", "24", "-t", "2", "-N", "40"]
+    ours, theirs = tmp_path / "ours.out", tmp_path / "ref.out"
+    r1 = subprocess.run([str(_native.CLI_PATH), *flags, "-o", str(ours)], capture_output=True, text=True)
+    assert r1.returncode == 0, r1.stderr
+    r2 = subprocess.run([str(REF_BIN), *flags, "-o", str(theirs)], capture_output=True, text=True)
+    assert r2.returncode == 0
+    h1, a = _parse(ours)
+    h2, b = _parse(theirs)
+    assert h1 == h2
+    assert h1[0].startswith("240\t")
+    np.testing.assert_allclose(a[:, 6], b[:, 6], rtol=1e-4, atol=0.011)
+    ours_set = {tuple(np.round(x[:6], 6)) for x in a}
+    gaps = np.abs(np.diff(b[:, 6]))
+    for n in range(1, len(b) - 1):
+        if gaps[n - 1] > 0.05 and gaps[n] > 0.05:
+            assert tuple(np.round(b[n, :6], 6)) in ours_set, b[n]

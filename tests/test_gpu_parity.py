@@ -50,6 +50,10 @@ def _setup(pairs, name, *extra):
     ("small", ("-F", "154", "-r", "24")),
     ("small", ("-F", "162", "-r", "24")),
     ("small", ("-F", "224", "-r", "24")),
+    # staged sizes (row and column launches)
+    ("small", ("-F", "256", "-r", "24")),
+    ("small", ("-F", "250", "-r", "24")),
+    ("c0", ("-F", "320", "-v", "0.9", "-r", "24")),
 ])
 def test_device_voxels_bit_exact(built, gpu, pairs, name, extra):
     from megadock_b200 import rotation_matrix
@@ -84,7 +88,9 @@ def test_device_voxels_vs_reference(built, gpu, pairs):
                                         ("small", ("-F", "80",)), ("small", ("-F", "112",)),
                                         ("small", ("-F", "48", "-v", "2.0")), ("small", ("-F", "88")),
                                         ("small", ("-F", "132")), ("small", ("-F", "90")), ("small", ("-F", "154")),
-                                        ("small", ("-F", "192")), ("small", ("-F", "224"))])
+                                        ("small", ("-F", "192")), ("small", ("-F", "224")),
+                                        ("small", ("-F", "240")), ("small", ("-F", "256")),
+                                        ("small", ("-F", "270")), ("c0", ("-F", "320", "-v", "0.9"))])
 def test_receptor_spectrum(built, gpu, pairs, name, extra):
     from oracle import oracle as O
     job, fp = _setup(pairs, name, *extra, "-r", "1")
@@ -165,6 +171,21 @@ def _check_rotation(got, rhat, job, r, t, m):
     ("small", ("-F", "200", "-r", "24"), 2, 2),
     ("small", ("-F", "216", "-r", "24"), 1, 2),
     ("small", ("-F", "220", "-r", "24"), 2, 2),
+    # staged sizes above 224 (the default grid table up to ng1 = 160)
+    ("small", ("-F", "240", "-r", "24"), 3, 2),
+    ("small", ("-F", "242", "-r", "24"), 1, 1),
+    ("small", ("-F", "250", "-r", "24"), 2, 1),
+    ("small", ("-F", "252", "-r", "24"), 3, 1),
+    ("small", ("-F", "256", "-r", "24"), 2, 2),
+    ("small", ("-F", "256", "-r", "24"), 20, 1),
+    ("small", ("-F", "264", "-r", "24"), 1, 1),
+    ("small", ("-F", "270", "-r", "24"), 3, 1),
+    ("small", ("-F", "280", "-r", "24"), 2, 1),
+    ("c0", ("-F", "288", "-r", "24"), 3, 1),
+    ("small", ("-F", "294", "-r", "24"), 1, 1),
+    ("small", ("-F", "300", "-r", "24"), 2, 1),
+    ("small", ("-F", "308", "-r", "24"), 3, 1),
+    ("c0", ("-F", "320", "-v", "0.9", "-r", "24"), 3, 2),
 ])
 def test_dock_matches_fp64_oracle(built, gpu, pairs, name, extra, t, nchk):
     from megadock_b200 import rotation_matrices
@@ -252,7 +273,7 @@ def test_batched_equals_plain(built, gpu, pairs):
 
 @pytest.mark.parametrize("extra", [("-F", "44", "-v", "2.5"), ("-F", "84"), ("-F", "132"), ("-F", "140"),
                                    ("-F", "50", "-v", "2.5"), ("-F", "110"), ("-F", "154"), ("-F", "192"),
-                                   ("-F", "224")])
+                                   ("-F", "224"), ("-F", "256"), ("-F", "250")])
 def test_batched_forms_at_table_sizes(built, gpu, pairs, extra):
     """The 11-smooth sizes: the batched graph (both lane counts, every tile)
     returns the plain form's records bit for bit; the other radix plans agree
@@ -274,7 +295,7 @@ def test_batched_forms_at_table_sizes(built, gpu, pairs, extra):
         assert np.all(np.abs(s1 - s0) <= 2 * (RTOL * np.abs(s0) + ATOL)), plan
 
 
-@pytest.mark.parametrize("extra", [("-F", "90"), ("-F", "154"), ("-F", "132"), ("-F", "224")])
+@pytest.mark.parametrize("extra", [("-F", "90"), ("-F", "154"), ("-F", "132"), ("-F", "224"), ("-F", "256")])
 def test_direct_pose_scores_at_table_sizes(built, gpu, pairs, extra):
     """The direct-sum rescoring (md_pose_scores, the adjoint's shift
     convention) gives the docking scores at their poses: the embedding

@@ -29,6 +29,10 @@ def _case(pairs, name, extra):
     ("c0", ("-F", "160", "-e", "2.5"), -45.0, 1.0, 2.5),
     ("c0", ("-F", "154"), -45.0, 1.0, 1.0),
     ("c0", ("-F", "224"), -45.0, 1.0, 1.0),
+    # ng1 above 112: the sweep's row masks (3 words) in global memory
+    ("c0", ("-F", "240"), -45.0, 1.0, 1.0),
+    ("c1", ("-F", "256", "-v", "0.9", "-e", "0.06"), -45.0, 1.0, 0.06),
+    ("c0", ("-F", "320", "-v", "0.6"), -45.0, 1.0, 1.0),
 ])
 def test_device_receptor_grids_bit_exact(built, gpu, pairs, name, extra, core, acer, elec):
     job, fp, xyz_c, rad, q, ace = _case(pairs, name, extra)
