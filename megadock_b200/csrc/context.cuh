@@ -374,6 +374,7 @@ const SizedOps *sized_ops_j(int N);
 const SizedOps *sized_ops_k(int N);
 const SizedOps *sized_ops_l(int N);
 const SizedOps *sized_ops_m(int N);
+const SizedOps *sized_ops_n(int N);
 
 inline const SizedOps *sized_ops(int N) {
     if (const SizedOps *o = sized_ops_a(N)) return o;
@@ -388,7 +389,8 @@ inline const SizedOps *sized_ops(int N) {
     if (const SizedOps *o = sized_ops_j(N)) return o;
     if (const SizedOps *o = sized_ops_k(N)) return o;
     if (const SizedOps *o = sized_ops_l(N)) return o;
-    return sized_ops_m(N);
+    if (const SizedOps *o = sized_ops_m(N)) return o;
+    return sized_ops_n(N);
 }
 
 }  // namespace mdb

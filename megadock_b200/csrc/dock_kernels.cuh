@@ -401,10 +401,20 @@ __global__ void __launch_bounds__(kNT0)
     for (int w = tid; w < 2 * NG * W; w += blockDim.x) dst[w] = (&cs[0][0])[w];
 }
 
-// Dynamic shared memory of k_vox_bits: the first charge entry of each cell.
+// Whether k_vox_bits keeps its bit planes (VoxShared) and output words in
+// dynamic shared memory: where their static form would pass 40 KB of the 48 KB
+// a kernel may declare statically (NG > 160).
+template <int NG>
+constexpr bool vox_bits_dyn() {
+    return sizeof(VoxShared<NG>) + sizeof(uint32_t) * 2 * NG * VoxShared<NG>::W > 40 * 1024;
+}
+
+// Dynamic shared memory of k_vox_bits: the first charge entry of each cell,
+// then (vox_bits_dyn) the bit planes and the output words.
 template <int NG>
 constexpr size_t vox_bits_smem() {
-    return sizeof(int) * NG * NG;
+    return sizeof(int) * NG * NG +
+           (vox_bits_dyn<NG>() ? sizeof(VoxShared<NG>) + sizeof(uint32_t) * 2 * NG * VoxShared<NG>::W : 0);
 }
 
 // PREMARKED: the marks come from K0m (marks != nullptr) instead of vox_mark.
@@ -415,10 +425,20 @@ __global__ void __launch_bounds__(kNT0)
                int2 *__restrict__ qlist, int *__restrict__ qcount, const uint32_t *__restrict__ marks = nullptr) {
     constexpr int W = VoxShared<NG>::W;
     constexpr int NBS = NG + 2 * kReach;
-    __shared__ VoxShared<NG> vs;
-    __shared__ uint32_t ob[2][NG * W];
     __shared__ int count;
-    extern __shared__ int first[];   // NG * NG (vox_bits_smem)
+    extern __shared__ __align__(16) int first[];   // NG * NG (vox_bits_smem)
+    VoxShared<NG> *vsp;
+    uint32_t(*ob)[NG * W];
+    if constexpr (vox_bits_dyn<NG>()) {
+        vsp = reinterpret_cast<VoxShared<NG> *>(first + NG * NG);
+        ob = reinterpret_cast<uint32_t(*)[NG * W]>(vsp + 1);
+    } else {
+        __shared__ VoxShared<NG> vs_static;
+        __shared__ uint32_t ob_static[2][NG * W];
+        vsp = &vs_static;
+        ob = ob_static;
+    }
+    VoxShared<NG> &vs = *vsp;
     const int p = blockIdx.x, b = blockIdx.y, tid = threadIdx.x;
     const bool gd = (L.delta != 1.0f);
     if constexpr (PREMARKED) {

@@ -314,6 +314,7 @@ MDB_PLAN(294, 14, 21)
 MDB_PLAN(300, 20, 15)
 MDB_PLAN(308, 28, 11)
 MDB_PLAN(320, 16, 20)
+MDB_PLAN(400, 20, 20)
 #undef MDB_PLAN
 
 // Whether the first passes of an axis of length N can skip the zero padding

@@ -35,9 +35,9 @@ def test_kernel_sizes_built(built):
               42, 50, 54, 66, 70, 90, 98, 110, 126, 150, 154,
               162, 168, 176, 180, 192, 196, 198, 200, 210, 216, 220, 224,
               # staged sizes: every 2 ng1 of the default grid table up to ng1 = 160
-              240, 242, 250, 252, 256, 264, 270, 280, 288, 294, 300, 308, 320):
+              240, 242, 250, 252, 256, 264, 270, 280, 288, 294, 300, 308, 320, 400):
         assert lib().md_fft_size_supported(n) == 1
-    for n in (46, 230, 244, 330, 400, 2048):
+    for n in (46, 230, 244, 330, 384, 2048):
         assert lib().md_fft_size_supported(n) == 0
 
 

@@ -54,6 +54,7 @@ def _setup(pairs, name, *extra):
     ("small", ("-F", "256", "-r", "24")),
     ("small", ("-F", "250", "-r", "24")),
     ("c0", ("-F", "320", "-v", "0.9", "-r", "24")),
+    ("c0", ("-F", "400", "-v", "0.75", "-r", "24")),   # class planes in dynamic shared memory
 ])
 def test_device_voxels_bit_exact(built, gpu, pairs, name, extra):
     from megadock_b200 import rotation_matrix
@@ -186,6 +187,7 @@ def _check_rotation(got, rhat, job, r, t, m):
     ("small", ("-F", "300", "-r", "24"), 2, 1),
     ("small", ("-F", "308", "-r", "24"), 3, 1),
     ("c0", ("-F", "320", "-v", "0.9", "-r", "24"), 3, 2),
+    ("c0", ("-F", "400", "-v", "0.75", "-r", "24"), 2, 1),
 ])
 def test_dock_matches_fp64_oracle(built, gpu, pairs, name, extra, t, nchk):
     from megadock_b200 import rotation_matrices

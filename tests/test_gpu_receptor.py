@@ -33,6 +33,7 @@ def _case(pairs, name, extra):
     ("c0", ("-F", "240"), -45.0, 1.0, 1.0),
     ("c1", ("-F", "256", "-v", "0.9", "-e", "0.06"), -45.0, 1.0, 0.06),
     ("c0", ("-F", "320", "-v", "0.6"), -45.0, 1.0, 1.0),
+    ("c0", ("-F", "400", "-v", "0.45"), -45.0, 1.0, 1.0),   # 4 mask words
 ])
 def test_device_receptor_grids_bit_exact(built, gpu, pairs, name, extra, core, acer, elec):
     job, fp, xyz_c, rad, q, ace = _case(pairs, name, extra)
