@@ -21,11 +21,11 @@ from __future__ import annotations
 
 _cache: dict = {}
 
-CANDIDATES = (4, 8, 16, 24, 32, 48, 64, 96, 128, 192)
+CANDIDATES = (4, 8, 16, 24, 32, 48, 64, 96, 128, 192, 256, 320, 384, 512)
 PLANS = (0, 1, 2)
 TILES = (32, 16, 8)
 LANES = (2, 1)
-WORK_BUDGET = 12 << 30
+WORK_BUDGET = 24 << 30   # of the B200's 180 GB
 
 
 def work_bytes_per_rotation(n: int) -> int:

@@ -167,3 +167,33 @@ def test_adjoint_rejects_bad_arguments(built, gpu, pairs):
         fp.adjoint_lse(mats, top1[:3], T, 1.0)
     with pytest.raises(ValueError):
         fp.adjoint_lse(mats, top1, T, 1.0, lig_rot=[24])
+
+
+def test_adjoint_at_a_staged_size(built, gpu, pairs):
+    """At N = 240 the ligand voxel grids of the adjoint come from the staged
+    row kernels: the device gradient equals the FP64 reference gradient taken
+    at the device's translations (24 rotations, every rotation's ligand grid
+    gradient checked for the heaviest one)."""
+    from megadock_b200 import rotation_matrices
+    from oracle import adjoint as A
+    job, fp = _setup(pairs, "small", "-F", "240", "-r", "24")
+    mats = rotation_matrices(job.rotation_angles())
+    fp.set_batch(8)
+    top1 = fp.cuda_fft(mats, t=1).copy()
+    shifts = np.stack([top1["i"], top1["j"], top1["k"]], -1).astype(np.int64)
+    scores = top1["score"].astype(np.float64)
+    _, w = A.weights(scores, T)
+    lig_rot = [int(np.argmax(w))]
+    dev = fp.adjoint_lse(mats, top1, T, 1.0, lig_rot=lig_rot)
+    rr, ri = job.receptor_grids()
+    xyz, rad, q = job.ligand_atoms()
+    ref = A.AdjointReference(rr, ri, xyz, rad, q, job.grid_width, job.grid_coord(), job.lig_core, job.nf1,
+                             fft=A.TorchFFT("cuda:0")).run(mats, shifts, scores, T, 1.0, lig_rot=lig_rot)
+    assert abs(dev["loss"] - ref["loss"]) <= 1e-12 * abs(ref["loss"])
+    for key in ("d_rec_r", "d_rec_i", "d_charge"):
+        d = np.abs(dev[key].astype(np.float64) - ref[key]).max()
+        assert d <= 1e-5 * np.abs(ref[key]).max(), (key, d)
+    for p, key in ((0, "d_lig_r"), (1, "d_lig_i")):
+        want = ref["d_lig"][lig_rot[0]][p]
+        assert np.abs(dev[key][0] - want).max() <= 1e-6 * max(np.abs(want).max(), 1e-30)
+    assert abs(dev["d_alpha"] - ref["d_alpha"]) <= 1e-5 * abs(ref["d_alpha"])

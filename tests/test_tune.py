@@ -54,8 +54,8 @@ def test_autotune_picks_the_fastest_shape_and_caches():
 def test_autotune_skips_batches_over_the_work_budget():
     from megadock_b200 import tune
     tune._cache.clear()
-    fp = FakeContext(160, best=(192, 0, 32))
+    fp = FakeContext(160, best=(512, 0, 32))
     per_rot = tune.work_bytes_per_rotation(160)
-    assert 128 * per_rot <= tune.WORK_BUDGET < 192 * per_rot
+    assert 320 * per_rot <= tune.WORK_BUDGET < 384 * per_rot
     b, _ = tune.autotune(fp, 0, 0, 3, sample=256, time_graph=lambda f: 1.0)
-    assert b == 128 and fp.released
+    assert b == 320 and fp.released
