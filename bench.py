@@ -583,14 +583,22 @@ def run_metric(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(local)
+    # collectives over NCCL, one GPU per rank; MD_BENCH_BACKEND=gloo runs them
+    # on host copies and lets ranks share GPUs (tests on a one-GPU machine)
+    backend = os.environ.get("MD_BENCH_BACKEND", "nccl")
+    gpu = local if backend == "nccl" else local % max(torch.cuda.device_count(), 1)
+    torch.cuda.set_device(gpu)
     dist = None
     if world > 1:
         import datetime
 
         import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                device_id=torch.device(f"cuda:{local}"))
+        if backend == "nccl":
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                    device_id=torch.device(f"cuda:{gpu}"))
+        else:
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+    coll = f"cuda:{gpu}" if backend == "nccl" else "cpu"   # where collective tensors live
 
     from megadock_b200 import POSE_DTYPE, FFTProcess, Job, rotation_matrices
     from megadock_b200.shard import gather_records, max_over_ranks, shard_range
@@ -598,9 +606,9 @@ def run_metric(args):
 
     # a dedicated stream: the library captures CUDA graphs on it, which the
     # legacy default stream does not allow
-    stream = torch.cuda.Stream(device=local)
+    stream = torch.cuda.Stream(device=gpu)
     torch.cuda.set_stream(stream)
-    dev = f"cuda:{local}"
+    dev = f"cuda:{gpu}"
     with tempfile.TemporaryDirectory() as tmp:
         rp, lp = make_inputs(tmp)
         config = workload_config(rp, lp)
@@ -613,7 +621,7 @@ def run_metric(args):
         # this rank's block of the one job (the whole job at one GPU)
         r0, r1 = shard_range(nrot, rank, world)
         nloc = r1 - r0
-        fp = FFTProcess(local, stream=stream.cuda_stream)
+        fp = FFTProcess(gpu, stream=stream.cuda_stream)
         fp.alloc_array(job.nf1, job.grid_width, job.grid_coord())
         fp.receptor_fft(rr, ri)
         fp.ligand_data_transfer_gpu(xyz, rad, q, job.lig_core)
@@ -645,7 +653,7 @@ def run_metric(args):
             torch.cuda.synchronize()
             ms = e0.elapsed_time(e1)
             if dist:
-                ms = max_over_ranks(ms, device=dev)
+                ms = max_over_ranks(ms, device=coll)
                 dist.barrier()
             return ms / steps
 
@@ -653,11 +661,11 @@ def run_metric(args):
             fp.dock_device(d_rot.data_ptr(), r0, nloc, T_POSES, d_pose.data_ptr())
             if dist:
                 # the job's exchange step: every rank's records, in rotation order
-                merged["all"] = gather_records(d_pose, nrot, T_POSES)
+                merged["all"] = gather_records(d_pose if coll != "cpu" else d_pose.cpu(), nrot, T_POSES)
 
         # batched, device-resident inputs
         fp.set_batch(batch)
-        with Clocks(local) as clk:
+        with Clocks(gpu) as clk:
             ms_batched = timed(dev_step, args.steps, args.warmup)
         all_rec = merged["all"] if dist else d_pose
         poses_timed = all_rec.cpu().numpy().view(POSE_DTYPE).copy() if rank == 0 else None
@@ -696,12 +704,12 @@ def run_metric(args):
         torch.cuda.synchronize()
         ms_e2e = 1000.0 * (time.perf_counter() - t0) / args.steps
         if dist:
-            ms_e2e = max_over_ranks(ms_e2e, device=dev)
+            ms_e2e = max_over_ranks(ms_e2e, device=coll)
         # per-stage profile of the batched form (events on the launch stream)
         stage_ms, launches_prof = fp.dock_profile(d_rot.data_ptr(), r0, nloc, T_POSES, d_pose.data_ptr())
         launches_all = launches_prof
         if dist:
-            t_l = torch.tensor([launches_prof], dtype=torch.int64, device=dev)
+            t_l = torch.tensor([launches_prof], dtype=torch.int64, device=coll)
             dist.all_reduce(t_l)
             launches_all = int(t_l.item())
         cufft = None
