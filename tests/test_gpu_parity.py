@@ -55,6 +55,7 @@ def _setup(pairs, name, *extra):
     ("small", ("-F", "250", "-r", "24")),
     ("c0", ("-F", "320", "-v", "0.9", "-r", "24")),
     ("c0", ("-F", "400", "-v", "0.75", "-r", "24")),   # class planes in dynamic shared memory
+    ("c0", ("-F", "256", "-b", "2.5", "-r", "24")),     # general core value, staged rows
 ])
 def test_device_voxels_bit_exact(built, gpu, pairs, name, extra):
     from megadock_b200 import rotation_matrix
@@ -188,6 +189,7 @@ def _check_rotation(got, rhat, job, r, t, m):
     ("small", ("-F", "308", "-r", "24"), 3, 1),
     ("c0", ("-F", "320", "-v", "0.9", "-r", "24"), 3, 2),
     ("c0", ("-F", "400", "-v", "0.75", "-r", "24"), 2, 1),
+    ("c0", ("-F", "256", "-b", "2.5", "-e", "0.06", "-r", "24"), 3, 1),
 ])
 def test_dock_matches_fp64_oracle(built, gpu, pairs, name, extra, t, nchk):
     from megadock_b200 import rotation_matrices
