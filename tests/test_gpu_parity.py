@@ -372,3 +372,34 @@ def test_plan_variants_agree(built, gpu, pairs, name, extra, t):
         same = (ref["i"] == got["i"]) & (ref["j"] == got["j"]) & (ref["k"] == got["k"])
         assert same.mean() >= 0.98, (plan, same.mean())
     fp.set_plan(0)
+
+
+def test_context_switches_between_resident_and_staged_sizes(built, gpu, pairs):
+    """One context docking at N = 128, then 256 (row and column launches, a
+    larger candidate buffer), then 128 again returns, each time, the records
+    of a fresh context of that size (batched form, graphs rebuilt)."""
+    from megadock_b200 import FFTProcess, Job, rotation_matrices
+    rp, lp = pairs["small"]
+    jobs = {n: Job(["-R", rp, "-L", lp, "-F", str(n), "-r", "24", "-t", "3"]) for n in (128, 256)}
+
+    def load(fp, job):
+        fp.alloc_array(job.nf1, job.grid_width, job.grid_coord())
+        rr, ri = job.receptor_grids()
+        fp.receptor_fft(rr, ri)
+        xyz, rad, q = job.ligand_atoms()
+        fp.ligand_data_transfer_gpu(xyz, rad, q, job.lig_core)
+
+    want = {}
+    for n, job in jobs.items():
+        fresh = FFTProcess(0)
+        load(fresh, job)
+        fresh.set_batch(8)
+        want[n] = fresh.cuda_fft(rotation_matrices(job.rotation_angles()), t=3).copy()
+        fresh.fft_memory_free()
+    fp = FFTProcess(0)
+    fp.set_batch(8)
+    for n in (128, 256, 128):
+        load(fp, jobs[n])
+        got = fp.cuda_fft(rotation_matrices(jobs[n].rotation_angles()), t=3)
+        assert np.array_equal(got, want[n]), n
+    fp.fft_memory_free()
