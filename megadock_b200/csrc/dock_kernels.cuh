@@ -535,12 +535,18 @@ __global__ void __launch_bounds__(kNT1, 1)
         __syncthreads();
     } else {
         const uint32_t *vb = vbits + ((size_t)b * NG + p) * 2 * NG * W;
-        for (int c = tid; c < NG * NG; c += blockDim.x) {
-            const int q = c / NG, s = c % NG;
-            const uint32_t bit = 1u << (s & 31);
-            const float v = (__ldg(&vb[q * W + (s >> 5)]) & bit) ? L.delta
-                            : (__ldg(&vb[NG * W + q * W + (s >> 5)]) & bit) ? 1.0f : 0.0f;
-            S[(q + OFF) * PITCH + s + OFF] = make_float2(v, 0.f);
+        // compile-time trip count, both class words loaded unconditionally
+        constexpr int CPT = (NG * NG + kNT1 - 1) / kNT1;
+#pragma unroll
+        for (int r = 0; r < CPT; ++r) {
+            const int c = tid + r * kNT1;
+            if (NG * NG % kNT1 == 0 || c < NG * NG) {
+                const int q = c / NG, s = c % NG;
+                const uint32_t bit = 1u << (s & 31);
+                const uint32_t w2 = __ldg(&vb[q * W + (s >> 5)]), w1 = __ldg(&vb[NG * W + q * W + (s >> 5)]);
+                const float v = (w2 & bit) ? L.delta : (w1 & bit) ? 1.0f : 0.0f;
+                S[(q + OFF) * PITCH + s + OFF] = make_float2(v, 0.f);
+            }
         }
         __syncthreads();
         const int nq = qcount[(size_t)b * NG + p];
@@ -677,12 +683,19 @@ __global__ void __launch_bounds__(kNT1B, fwd_cb_fits<N>() ? 2 : 1)
         __syncthreads();
     } else {
         const uint32_t *vb = vbits + ((size_t)b * NG + p) * 2 * NG * W;
-        for (int c = tid; c < NG * NG; c += blockDim.x) {
-            const int q = c / NG, s = c % NG;
-            const uint32_t bit = 1u << (s & 31);
-            const float v = (__ldg(&vb[q * W + (s >> 5)]) & bit) ? L.delta
-                            : (__ldg(&vb[NG * W + q * W + (s >> 5)]) & bit) ? 1.0f : 0.0f;
-            Z[q * PZ + s + OFF] = make_float2(v, 0.f);
+        // the cells of this thread with a compile-time trip count and both
+        // class words loaded unconditionally: all loads in flight at once
+        constexpr int CPT = (NG * NG + kNT1B - 1) / kNT1B;
+#pragma unroll
+        for (int r = 0; r < CPT; ++r) {
+            const int c = tid + r * kNT1B;
+            if (NG * NG % kNT1B == 0 || c < NG * NG) {
+                const int q = c / NG, s = c % NG;
+                const uint32_t bit = 1u << (s & 31);
+                const uint32_t w2 = __ldg(&vb[q * W + (s >> 5)]), w1 = __ldg(&vb[NG * W + q * W + (s >> 5)]);
+                const float v = (w2 & bit) ? L.delta : (w1 & bit) ? 1.0f : 0.0f;
+                Z[q * PZ + s + OFF] = make_float2(v, 0.f);
+            }
         }
         __syncthreads();
         const int nq = qcount[(size_t)b * NG + p];
