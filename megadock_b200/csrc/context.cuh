@@ -220,6 +220,7 @@ struct Sized {
         set((const void *)k_xline_herm<N, 32>, smem_xline<32>());
         set((const void *)k_xline_herm<N, 16>, smem_xline<16>());
         set((const void *)k_xline_herm<N, 8>, smem_xline<8>());
+        if constexpr (xline_fold_ok<N>()) set((const void *)k_xline_fold<N, 16>, smem_xline<16>());
         if (e == cudaSuccess) done = true;
         return e;
     }
@@ -325,7 +326,9 @@ struct Sized {
         if (ev) cudaEventRecord(ev[1], s);
         any_fwd<0>(s, nb, L, G, w.vbits, w.qlist, w.qcount, nullptr, nullptr, w.A, nullptr, nullptr);
         if (ev) cudaEventRecord(ev[2], s);
-        if (c->tile == 16)
+        if (c->tile == 16 && xline_fold_ok<N>())
+            k_xline_fold<N, 16><<<dim3(NH * ((N + 15) / 16), nb), 256, smem_xline<16>(), s>>>(G, w.A, c->d_Rh, w.G);
+        else if (c->tile == 16)
             k_xline_herm<N, 16><<<dim3(NH * ((N + 15) / 16), nb), 256, smem_xline<16>(), s>>>(G, w.A, c->d_Rh, w.G);
         else if (c->tile == 8)
             k_xline_herm<N, 8><<<dim3(NH * ((N + 7) / 8), nb), 128, smem_xline<8>(), s>>>(G, w.A, c->d_Rh, w.G);

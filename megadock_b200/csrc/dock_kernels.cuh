@@ -1011,6 +1011,187 @@ __global__ void __launch_bounds__(16 * LT, xline_occ<N>() / LT)
     }
 }
 
+// K2, register-fold form.  The same transform as k_xline_herm with the
+// forward split reversed (pass 1 a DFT-F1 over stride F2, pass 2 a DFT-F2
+// whose outputs sit at kx = u + F1 k2): the conjugate partner -kx of every
+// output of the own item u is an output of the mirror item (F1 - u) mod F1,
+// so one thread transforms both, multiplies both by conj(R^), folds them into
+// H in registers, and runs the first inverse pass (a DFT-F2 over the same
+// stride F1, the inverse split being F2 x F1) before anything is stored.  The
+// mirror tile's products never go back to shared memory, and the fold and
+// the first inverse pass need no barrier of their own: three barriers per
+// pass instead of five.
+template <int N>
+struct FoldPlan {
+    static constexpr int F1 = Plan<N>::R2, F2 = Plan<N>::R1;
+};
+// Used for the 16-line tiles at N = 128, compiled for four 256-thread CTAs
+// per SM (64 registers).  B200, 13,824 of the 54,000 rotations at 512 per
+// launch: 237.4 ms per 54,000 rotations against 262.8 for k_xline_herm; at
+// five CTAs per SM (48 registers, 100 bytes of spills) 284.0, at three 267.2.
+template <int N>
+constexpr bool xline_fold_ok() {
+    return N == 128;
+}
+template <int N>
+constexpr int xline_fold_occ() {
+    return 64;
+}
+
+template <int N, int LT = kLT>
+__global__ void __launch_bounds__(16 * LT, xline_fold_occ<N>() / LT)
+    k_xline_fold(GridView G, const float2 *__restrict__ A, const float2 *__restrict__ Rh, float2 *__restrict__ Gh) {
+    constexpr int NG = N / 2, NH = N / 2, OFF = N / 4;
+    constexpr int F1 = FoldPlan<N>::F1, F2 = FoldPlan<N>::F2;
+    constexpr bool PR = N % 4 == 0 && F1 % 4 == 0;
+    constexpr int TILES = (N + LT - 1) / LT;
+    constexpr int NT = 16 * LT;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    float2 *X0 = reinterpret_cast<float2 *>(smem_raw);   // own tile   [N][LT]
+    float2 *X1 = X0 + N * LT;                           // mirror tile [N][LT]
+    float2 *TWs = X1 + N * LT;                          // twiddles W_N^j (xline_tw_smem)
+    if constexpr (xline_tw_smem<N>()) {
+        for (int e = threadIdx.x; e < N; e += NT) TWs[e] = __ldg(&G.tw[e]);
+        __syncthreads();
+    }
+    auto tw_at = [&](int j) {
+        if constexpr (xline_tw_smem<N>()) return TWs[j];
+        else return __ldg(&G.tw[j]);
+    };
+    const int lane = threadIdx.x % LT;
+    const int ky = blockIdx.x / TILES;
+    const int kz = (blockIdx.x % TILES) * LT + lane;
+    const bool ok = kz < N;
+    const int kzm = (N - kz) % N;
+    const int b = blockIdx.y;
+    const float2 *Ab = A + (size_t)b * NG * N * N;
+    float2 *Gb = Gh + (size_t)b * N * NH * N;
+    const int passes = (ky == 0) ? 2 : 1;
+
+    for (int pass = 0; pass < passes; ++pass) {
+        const int kyo = pass == 0 ? ky : NH;   // own row
+        const int kym = (N - kyo) % N;         // mirror row
+        // forward pass 1 (DFT-F1 over stride F2) on both tiles, straight from
+        // global (pruned rows), every load of a thread issued before its DFTs
+        constexpr int IT1 = (2 * LT * F2 + NT - 1) / NT;
+        float2 v1[IT1][F1];
+#pragma unroll
+        for (int r = 0; r < IT1; ++r) {
+            const int it = threadIdx.x + r * NT;
+            const int s = it / (LT * F2);
+            const int t = (it / LT) % F2;
+            const int row = s ? kym : kyo, col = s ? kzm : kz;
+            const bool live = ok && it < 2 * LT * F2;
+            static_for<0, F1>([&](auto m_) {
+                constexpr int mm = decltype(m_)::value;
+                const int pp = t + F2 * mm - OFF;   // spectrum plane of x = t + F2 mm, if any
+                if constexpr (PR && (mm < F1 / 4 || mm >= 3 * F1 / 4)) {
+                    v1[r][mm] = make_float2(0.f, 0.f);
+                } else if constexpr (PR) {
+                    v1[r][mm] = live ? Ab[((size_t)pp * N + row) * N + col] : make_float2(0.f, 0.f);
+                } else {
+                    v1[r][mm] = (live && (unsigned)pp < (unsigned)NG) ? Ab[((size_t)pp * N + row) * N + col]
+                                                                     : make_float2(0.f, 0.f);
+                }
+            });
+        }
+#pragma unroll
+        for (int r = 0; r < IT1; ++r) {
+            const int it = threadIdx.x + r * NT;
+            if (it < 2 * LT * F2) {
+                const int s = it / (LT * F2);
+                const int t = (it / LT) % F2;
+                Dft<F1, -1>::run(v1[r]);
+                float2 *X = s ? X1 : X0;
+                static_for<0, F1>([&](auto k1_) {
+                    constexpr int k1 = decltype(k1_)::value;
+                    float2 x = v1[r][k1];
+                    if constexpr (k1 != 0) x = cmul(x, tw_at(t * k1));
+                    X[(k1 * F2 + t) * LT + lane] = x;
+                });
+            }
+        }
+        __syncthreads();
+        // forward pass 2 of the own item u and the mirror item (F1 - u) mod F1,
+        // conj(R^) products, H = (P_own(kx) + conj P_mirror(-kx)) / 2 and the
+        // first inverse pass, in registers
+        constexpr int IT2 = (LT * F1 + NT - 1) / NT;
+        float2 h[IT2][F2];
+#pragma unroll
+        for (int r = 0; r < IT2; ++r) {
+            const int it = threadIdx.x + r * NT;
+            if (it < LT * F1) {
+                const int u = it / LT;
+                const int um = (F1 - u) % F1;
+                float2 pm[F2];
+                static_for<0, F2>([&](auto n2_) {
+                    constexpr int n2 = decltype(n2_)::value;
+                    h[r][n2] = X0[(u * F2 + n2) * LT + lane];
+                    pm[n2] = X1[(um * F2 + n2) * LT + lane];
+                });
+                Dft<F2, -1>::run(h[r]);
+                Dft<F2, -1>::run(pm);
+                static_for<0, F2>([&](auto k2_) {
+                    constexpr int k2 = decltype(k2_)::value;
+                    const float2 rov = ok ? __ldg(&Rh[((size_t)(u + F1 * k2) * N + kyo) * N + kz]) : make_float2(0.f, 0.f);
+                    const float2 rm = ok ? __ldg(&Rh[((size_t)(um + F1 * k2) * N + kym) * N + kzm]) : make_float2(0.f, 0.f);
+                    h[r][k2] = cmulconj(rov, h[r][k2]);
+                    pm[k2] = cmulconj(rm, pm[k2]);
+                });
+                // the partner of kx = u + F1 k2 is mirror output (F2 - 1 - k2)
+                // for u > 0 and (F2 - k2) mod F2 for u = 0
+                if (u == 0) {
+                    static_for<0, F2>([&](auto k2_) {
+                        constexpr int k2 = decltype(k2_)::value, j2 = (F2 - k2) % F2;
+                        h[r][k2] = make_float2(0.5f * (h[r][k2].x + pm[j2].x), 0.5f * (h[r][k2].y - pm[j2].y));
+                    });
+                } else {
+                    static_for<0, F2>([&](auto k2_) {
+                        constexpr int k2 = decltype(k2_)::value, j2 = F2 - 1 - k2;
+                        h[r][k2] = make_float2(0.5f * (h[r][k2].x + pm[j2].x), 0.5f * (h[r][k2].y - pm[j2].y));
+                    });
+                }
+                Dft<F2, +1>::run(h[r]);
+                static_for<1, F2>([&](auto k1_) {
+                    constexpr int k1 = decltype(k1_)::value;
+                    h[r][k1] = cmul(h[r][k1], conjf2(tw_at(u * k1)));
+                });
+            }
+        }
+        __syncthreads();
+#pragma unroll
+        for (int r = 0; r < IT2; ++r) {
+            const int it = threadIdx.x + r * NT;
+            if (it < LT * F1) {
+                const int u = it / LT;
+                static_for<0, F2>([&](auto k1) { X0[(k1 * F1 + u) * LT + lane] = h[r][k1]; });
+            }
+        }
+        __syncthreads();
+        // inverse pass 2 (DFT-F1 over items u2 < F2) -> Gh (row 0 packs ky = 0 and ky = N/2)
+        for (int it = threadIdx.x; it < LT * F2; it += NT) {
+            const int u2 = it / LT;
+            float2 o[F1];
+            static_for<0, F1>([&](auto n2) { o[decltype(n2)::value] = X0[(u2 * F1 + decltype(n2)::value) * LT + lane]; });
+            Dft<F1, +1>::run(o);
+            if (ok) {
+                static_for<0, F1>([&](auto k2) {
+                    const int x = u2 + F2 * k2;
+                    float2 *dst = &Gb[((size_t)x * NH + ky) * N + kz];
+                    if (ky != 0 || pass == 0) {
+                        *dst = o[k2];
+                    } else {
+                        // same thread wrote the ky = 0 value in pass 0
+                        const float2 g0 = *dst;
+                        *dst = make_float2(g0.x - o[k2].y, g0.y + o[k2].x);
+                    }
+                });
+            }
+        }
+        if (passes > 1) __syncthreads();
+    }
+}
+
 // ------------------------------------------------------------------ K3
 // Selection order for top-t: larger key first, then smaller linear index.
 // NaN keys are never selected (they fail every comparison in the reference).
@@ -1134,6 +1315,13 @@ constexpr size_t c2r_smem() {
     return (size_t)(N / 2) * (PA > PB ? PA : PB) * sizeof(float2);
 }
 
+// Whether the plane kernel folds the half spectrum inside pass 1 of its ky
+// transform (both splits of the ky axis even).
+template <int N, int V>
+constexpr bool c2r_fold_ok() {
+    return N == 128 && C2RPlan<N, V>::Q1 % 2 == 0 && C2RPlan<N, V>::Q2 % 2 == 0;
+}
+
 template <int N, int T, int V = 0>
 constexpr int c2r_min_blocks() {
     using P = C2RPlan<N, V>;
@@ -1168,8 +1356,13 @@ __global__ void __launch_bounds__(kNT, c2r_min_blocks<N, T, V>())
     const int tid = threadIdx.x;
     const float2 *Gp = Gh + ((size_t)b * N + x) * NH * N;
 
+    // The z pass works on whole rows.  Where the rows split evenly over the
+    // warps (WZ), warp w owns rows [w NH/16, (w+1) NH/16) in both of its
+    // passes, so the passes are separated by warp barriers only; the plane
+    // barrier comes once, before the ky pass reads across rows.
+    constexpr bool WZ = kNT == 512 && NH % 16 == 0 && (NH / 16 * R2) % 32 == 0 && (NH / 16 * R1) % 32 == 0;
     // (1a) inverse kz pass 1, straight from global: item = (row, t), t fastest
-    MDB_K3_ITEMS(it, NH * R2) {
+    auto z_pass1 = [&](int it) {
         const int row = it / R2, t = it % R2;
         float2 v[R1];
         static_for<0, R1>([&](auto m_) {
@@ -1183,16 +1376,26 @@ __global__ void __launch_bounds__(kNT, c2r_min_blocks<N, T, V>())
             if constexpr (k1 != 0) xv = cmul(xv, conjf2(tw_at(t * k1)));
             S[row * PITCH + k1 * (R2 + 1) + t] = xv;
         });
+    };
+    if constexpr (WZ) {
+        constexpr int IPW = NH / 16 * R2;
+#pragma unroll
+        for (int r = 0; r < IPW / 32; ++r) z_pass1((tid >> 5) * IPW + (tid & 31) + 32 * r);
+        __syncwarp();
+    } else {
+        MDB_K3_ITEMS(it, NH * R2) { z_pass1(it); }
+        __syncthreads();
     }
-    __syncthreads();
     // (1b) inverse kz pass 2: item = (row, u), u fastest; natural order after a barrier
     {
-        constexpr int IPT = (NH * R1 + kNT - 1) / kNT;
+        constexpr int IPW = WZ ? NH / 16 * R1 : 0;
+        constexpr int IPT = WZ ? IPW / 32 : (NH * R1 + kNT - 1) / kNT;
+        auto item = [&](int r) { return WZ ? (tid >> 5) * IPW + (tid & 31) + 32 * r : tid + r * kNT; };
         float2 reg[IPT][R2];
 #pragma unroll
         for (int r = 0; r < IPT; ++r) {
-            const int it = tid + r * kNT;
-            if (it < NH * R1) {
+            const int it = item(r);
+            if (WZ || it < NH * R1) {
                 const int row = it / R1, u = it % R1;
                 static_for<0, R2>([&](auto n2_) {
                     constexpr int n2 = decltype(n2_)::value;
@@ -1201,55 +1404,145 @@ __global__ void __launch_bounds__(kNT, c2r_min_blocks<N, T, V>())
                 Dft<R2, +1>::run(reg[r]);
             }
         }
-        __syncthreads();
+        if constexpr (WZ) __syncwarp();
+        else __syncthreads();
 #pragma unroll
         for (int r = 0; r < IPT; ++r) {
-            const int it = tid + r * kNT;
-            if (it < NH * R1) {
+            const int it = item(r);
+            if (WZ || it < NH * R1) {
                 const int row = it / R1, u = it % R1;
                 static_for<0, R2>([&](auto k2) { S[row * PITCH + u + R1 * k2] = reg[r][k2]; });
             }
         }
     }
     __syncthreads();
-    // (2a) fold the half spectrum into Z, in place (pairs k, N/2-k)
-    MDB_K3_ITEMS(it, N * (NH / 2 + 1)) {
-        const int z = it % N, k = it / N;
-        if (k == 0) {
-            const float2 v = S[z];   // X0 + i X_{N/2}, both real
-            S[z] = make_float2(v.x + v.y, v.x - v.y);
-        } else {
-            const int k2 = NH - k;
-            const float2 a = S[k * PITCH + z], c = S[k2 * PITCH + z];
-            const float2 wk = conjf2(tw_at(k)), wk2 = conjf2(tw_at(k2));
-            // E = a + conj(c), D = a - conj(c), Z = E + i w^k D
+    if constexpr (c2r_fold_ok<N, V>()) {
+        // (2a + 2b) the fold into Z and pass 1 of the N/2-point inverse along
+        // ky in one item.  Pass 1 item tt reads and writes the rows
+        // tt + Q2 m; the fold partner N/2 - k of row k = tt + Q2 m is row
+        // (Q2 - tt) + Q2 (Q1 - 1 - m) for tt > 0, so item g takes the row
+        // sets tt = g and Q2 - g, and item 0 the two sets that pair with
+        // themselves (tt = 0: Q2 m with Q2 (Q1 - m), row 0 packed; tt = Q2/2).
+        // Each item reads and writes only its own rows: no barrier between
+        // the fold and the pass.
+        // Z_k = E + i w^k D, E = a + conj c, D = a - conj c, a = X_k, c = X_{N/2-k};
+        // w^{N/2-k} = -conj(w^k).  The folded rows go back to their own slots
+        // (eight values in registers at a time, which keeps the kernel at 40
+        // registers without spills) and each row set is then reloaded for its
+        // DFT.  B200, N = 128, 13,824 of the 54,000 rotations at 512 per
+        // launch, with the warp-owned z pass above: 274.3 ms per 54,000
+        // rotations against 287.7 for the separate fold pass; holding both
+        // row sets in registers spilled and took 298.0.
+        auto zpair = [&](float2 &a, float2 &c, int k) {
+            const float2 w = conjf2(tw_at(k));
+            const float2 w2 = make_float2(-w.x, w.y);
             const float2 e1 = make_float2(a.x + c.x, a.y - c.y), d1 = make_float2(a.x - c.x, a.y + c.y);
-            const float2 o1 = cmul(wk, d1);
-            const float2 z1 = make_float2(e1.x - o1.y, e1.y + o1.x);
-            if (k2 != k) {
-                const float2 e2 = make_float2(c.x + a.x, c.y - a.y), d2 = make_float2(c.x - a.x, c.y + a.y);
-                const float2 o2 = cmul(wk2, d2);
-                S[k2 * PITCH + z] = make_float2(e2.x - o2.y, e2.y + o2.x);
+            const float2 e2 = make_float2(c.x + a.x, c.y - a.y), d2 = make_float2(c.x - a.x, c.y + a.y);
+            const float2 o1 = cmul(w, d1), o2 = cmul(w2, d2);
+            a = make_float2(e1.x - o1.y, e1.y + o1.x);
+            c = make_float2(e2.x - o2.y, e2.y + o2.x);
+        };
+        MDB_K3_ITEMS(it, N * (Q2 / 2)) {
+            const int z = it % N, g = it / N;
+            const int ta = g, tb = g == 0 ? Q2 / 2 : Q2 - g;
+            auto row = [&](int r) -> float2 & { return S[r * PITCH + z]; };
+            if (g == 0) {
+                float2 v[Q1];
+                static_for<0, Q1>([&](auto m_) { v[decltype(m_)::value] = row(Q2 * decltype(m_)::value); });
+                v[0] = make_float2(v[0].x + v[0].y, v[0].x - v[0].y);
+                static_for<1, Q1 / 2 + 1>([&](auto m_) {
+                    constexpr int mm = decltype(m_)::value;
+                    if constexpr (2 * mm == Q1) {
+                        float2 c = v[mm];
+                        zpair(v[mm], c, Q2 * mm);
+                    } else {
+                        zpair(v[mm], v[Q1 - mm], Q2 * mm);
+                    }
+                });
+                static_for<0, Q1>([&](auto m_) { row(Q2 * decltype(m_)::value) = v[decltype(m_)::value]; });
+                asm volatile("" ::: "memory");
+                static_for<0, Q1>([&](auto m_) { v[decltype(m_)::value] = row(Q2 / 2 + Q2 * decltype(m_)::value); });
+                static_for<0, Q1 / 2>([&](auto m_) {
+                    constexpr int mm = decltype(m_)::value;
+                    zpair(v[mm], v[Q1 - 1 - mm], Q2 / 2 + Q2 * mm);
+                });
+                static_for<0, Q1>([&](auto m_) { row(Q2 / 2 + Q2 * decltype(m_)::value) = v[decltype(m_)::value]; });
+            } else {
+                static_for<0, 2>([&](auto h_) {
+                    constexpr int h = decltype(h_)::value;
+                    float2 a[Q1 / 2], c[Q1 / 2];
+                    static_for<0, Q1 / 2>([&](auto j_) {
+                        constexpr int j = decltype(j_)::value, mm = h * (Q1 / 2) + j;
+                        a[j] = row(ta + Q2 * mm);
+                        c[j] = row(tb + Q2 * (Q1 - 1 - mm));
+                    });
+                    static_for<0, Q1 / 2>([&](auto j_) {
+                        constexpr int j = decltype(j_)::value, mm = h * (Q1 / 2) + j;
+                        zpair(a[j], c[j], ta + Q2 * mm);
+                    });
+                    static_for<0, Q1 / 2>([&](auto j_) {
+                        constexpr int j = decltype(j_)::value, mm = h * (Q1 / 2) + j;
+                        row(ta + Q2 * mm) = a[j];
+                        row(tb + Q2 * (Q1 - 1 - mm)) = c[j];
+                    });
+                    asm volatile("" ::: "memory");
+                });
             }
-            S[k * PITCH + z] = z1;
+            asm volatile("" ::: "memory");
+            static_for<0, 2>([&](auto s_) {
+                const int tt = decltype(s_)::value == 0 ? ta : tb;
+                float2 v[Q1];
+                static_for<0, Q1>([&](auto m_) { v[decltype(m_)::value] = row(tt + Q2 * decltype(m_)::value); });
+                Dft<Q1, +1>::run(v);
+                static_for<0, Q1>([&](auto k1_) {
+                    constexpr int k1 = decltype(k1_)::value;
+                    float2 xv = v[k1];
+                    if constexpr (k1 != 0) xv = cmul(xv, conjf2(tw_at(2 * tt * k1)));
+                    row(k1 * Q2 + tt) = xv;
+                });
+                asm volatile("" ::: "memory");
+            });
         }
-    }
-    __syncthreads();
-    // (2b) N/2-point inverse along ky, pass 1 (lanes = z), in place
-    MDB_K3_ITEMS(it, N * Q2) {
-        const int z = it % N, tt = it / N;
-        float2 v[Q1];
-        static_for<0, Q1>([&](auto m_) {
-            constexpr int mm = decltype(m_)::value;
-            v[mm] = S[(tt + Q2 * mm) * PITCH + z];
-        });
-        Dft<Q1, +1>::run(v);
-        static_for<0, Q1>([&](auto k1_) {
-            constexpr int k1 = decltype(k1_)::value;
-            float2 xv = v[k1];
-            if constexpr (k1 != 0) xv = cmul(xv, conjf2(tw_at(2 * tt * k1)));
-            S[(k1 * Q2 + tt) * PITCH + z] = xv;
-        });
+    } else {
+        // (2a) fold the half spectrum into Z, in place (pairs k, N/2-k)
+        MDB_K3_ITEMS(it, N * (NH / 2 + 1)) {
+            const int z = it % N, k = it / N;
+            if (k == 0) {
+                const float2 v = S[z];   // X0 + i X_{N/2}, both real
+                S[z] = make_float2(v.x + v.y, v.x - v.y);
+            } else {
+                const int k2 = NH - k;
+                const float2 a = S[k * PITCH + z], c = S[k2 * PITCH + z];
+                const float2 wk = conjf2(tw_at(k)), wk2 = conjf2(tw_at(k2));
+                // E = a + conj(c), D = a - conj(c), Z = E + i w^k D
+                const float2 e1 = make_float2(a.x + c.x, a.y - c.y), d1 = make_float2(a.x - c.x, a.y + c.y);
+                const float2 o1 = cmul(wk, d1);
+                const float2 z1 = make_float2(e1.x - o1.y, e1.y + o1.x);
+                if (k2 != k) {
+                    const float2 e2 = make_float2(c.x + a.x, c.y - a.y), d2 = make_float2(c.x - a.x, c.y + a.y);
+                    const float2 o2 = cmul(wk2, d2);
+                    S[k2 * PITCH + z] = make_float2(e2.x - o2.y, e2.y + o2.x);
+                }
+                S[k * PITCH + z] = z1;
+            }
+        }
+        __syncthreads();
+        // (2b) N/2-point inverse along ky, pass 1 (lanes = z), in place
+        MDB_K3_ITEMS(it, N * Q2) {
+            const int z = it % N, tt = it / N;
+            float2 v[Q1];
+            static_for<0, Q1>([&](auto m_) {
+                constexpr int mm = decltype(m_)::value;
+                v[mm] = S[(tt + Q2 * mm) * PITCH + z];
+            });
+            Dft<Q1, +1>::run(v);
+            static_for<0, Q1>([&](auto k1_) {
+                constexpr int k1 = decltype(k1_)::value;
+                float2 xv = v[k1];
+                if constexpr (k1 != 0) xv = cmul(xv, conjf2(tw_at(2 * tt * k1)));
+                S[(k1 * Q2 + tt) * PITCH + z] = xv;
+            });
+        }
     }
     __syncthreads();
     // (2c) pass 2 -> scores s[2m], s[2m+1] -> per-thread top-T
