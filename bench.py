@@ -748,7 +748,7 @@ def run_metric(args):
     # dram__bytes_write.sum per launch / 64, profiles/ncu_dock_kernels_n128_b64.md);
     # scaled by rotations per launch (R^, read once per launch by xline, adds
     # 16.8 MB per launch and is left in the xline figure)
-    traffic_per_rotation = {"voxelize": 79.4e3, "plane_fwd": 7.54e6, "xline": 17.07e6, "plane_inv": 8.47e6,
+    traffic_per_rotation = {"voxelize": 79.4e3, "plane_fwd": 7.54e6, "xline": 17.08e6, "plane_inv": 8.45e6,
                             "merge": 3.3e3}
     traffic = traffic_per_rotation[names[dom]] * batch if N_FFT == 128 else None
     value = nrot / (ms_batched * 1e-3)
