@@ -1204,6 +1204,20 @@ struct Cand {
     int idx;
 };
 
+// Order-preserving integer image of a key for the warp reductions of the
+// plane kernel (redux.sync reduces integers in one instruction where a
+// shuffle tree takes five dependent steps): larger keys map to larger
+// integers, -0 and +0 to the same one (they compare equal), NaN below every
+// key.
+__device__ __forceinline__ int key_ord(float k) {
+    if (k != k) return INT_MIN;
+    const int b = __float_as_int(k == 0.f ? 0.f : k);
+    return b >= 0 ? b : b ^ 0x7FFFFFFF;
+}
+__device__ __forceinline__ float ord_key(int o) {
+    return __int_as_float(o >= 0 ? o : o ^ 0x7FFFFFFF);
+}
+
 // Block-wide best candidate; idx < 0 means "none".
 __device__ __forceinline__ Cand block_best(Cand mine, Cand *red) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -1611,11 +1625,14 @@ __global__ void __launch_bounds__(kNT, c2r_min_blocks<N, T, V>())
             const int lane = tid & 31, warp = tid >> 5;
             float v = tmax, thw = -INFINITY;
             for (int r = 0; r < nsel; ++r) {
-                float m = v;
-#pragma unroll
-                for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
-                thw = m;
-                const unsigned holders = __ballot_sync(0xffffffffu, v == m);
+                const int vo = key_ord(v);
+                const int mo = __reduce_max_sync(0xffffffffu, vo);
+                if (mo == INT_MIN) {   // every lane NaN: no bound from this warp
+                    thw = NAN;
+                    break;
+                }
+                thw = ord_key(mo);
+                const unsigned holders = __ballot_sync(0xffffffffu, vo == mo);
                 if (lane == __ffs(holders) - 1) v = -INFINITY;
             }
             if (lane == 0) thr_w[warp] = thw;
@@ -1639,28 +1656,27 @@ __global__ void __launch_bounds__(kNT, c2r_min_blocks<N, T, V>())
             }
         }
     }
-    // merge: each warp takes its best nsel from its lanes' lists (shuffles
-    // only), then warp 0 takes the plane's best nsel from the warps' lists,
-    // with one block barrier in between
+    // merge: each warp takes its best nsel from its lanes' lists (warp
+    // reductions only), then warp 0 takes the plane's best nsel from the
+    // warps' lists, with one block barrier in between
     __shared__ Cand wl[kNT / 32][16];
     const int lane = tid & 31, warp = tid >> 5;
+    // The lanes' best candidate in selection order (larger key, then smaller
+    // cell index; cell indices are distinct): the largest key by one integer
+    // reduction, the smallest index among the lanes holding it by another.
     auto warp_best = [&](Cand c, int &owner) {
-        owner = lane;
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            const float k2 = __shfl_down_sync(0xffffffffu, c.key, o);
-            const int i2 = __shfl_down_sync(0xffffffffu, c.idx, o);
-            const int w2 = __shfl_down_sync(0xffffffffu, owner, o);
-            if (i2 >= 0 && (c.idx < 0 || key_better(k2, i2, c.key, c.idx))) {
-                c.key = k2;
-                c.idx = i2;
-                owner = w2;
-            }
+        const bool valid = c.idx >= 0;
+        const int ko = valid ? key_ord(c.key) : INT_MIN;
+        const int kmax = __reduce_max_sync(0xffffffffu, ko);
+        const bool tie = valid && ko == kmax;
+        const int imin = __reduce_min_sync(0xffffffffu, tie ? c.idx : INT_MAX);
+        const unsigned win = __ballot_sync(0xffffffffu, tie && c.idx == imin);
+        if (win == 0) {   // no lane holds a candidate
+            owner = 0;
+            return Cand{0.f, -1};
         }
-        c.key = __shfl_sync(0xffffffffu, c.key, 0);
-        c.idx = __shfl_sync(0xffffffffu, c.idx, 0);
-        owner = __shfl_sync(0xffffffffu, owner, 0);
-        return c;
+        owner = __ffs(win) - 1;
+        return Cand{__shfl_sync(0xffffffffu, c.key, owner), imin};
     };
     if (__any_sync(0xffffffffu, top.i[0] != INT_MAX)) {
         for (int r = 0; r < nsel; ++r) {
