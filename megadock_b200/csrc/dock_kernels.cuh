@@ -1218,32 +1218,37 @@ __device__ __forceinline__ float ord_key(int o) {
     return __int_as_float(o >= 0 ? o : o ^ 0x7FFFFFFF);
 }
 
+// The best candidate of a warp's lanes in selection order (larger key, then
+// smaller cell index; the lanes' cell indices are distinct), broadcast to
+// every lane, and the lane that holds it; idx < 0 when no lane holds one.
+// The largest key comes from one integer reduction over the keys'
+// order-preserving images, the smallest index among its holders from a
+// second.
+__device__ __forceinline__ Cand warp_best(Cand c, int &owner) {
+    const bool valid = c.idx >= 0;
+    const int ko = valid ? key_ord(c.key) : INT_MIN;
+    const int kmax = __reduce_max_sync(0xffffffffu, ko);
+    const bool tie = valid && ko == kmax;
+    const int imin = __reduce_min_sync(0xffffffffu, tie ? c.idx : INT_MAX);
+    const unsigned win = __ballot_sync(0xffffffffu, tie && c.idx == imin);
+    if (win == 0) {
+        owner = 0;
+        return Cand{0.f, -1};
+    }
+    owner = __ffs(win) - 1;
+    return Cand{__shfl_sync(0xffffffffu, c.key, owner), imin};
+}
+
 // Block-wide best candidate; idx < 0 means "none".
 __device__ __forceinline__ Cand block_best(Cand mine, Cand *red) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        const float k2 = __shfl_down_sync(0xffffffffu, mine.key, o);
-        const int i2 = __shfl_down_sync(0xffffffffu, mine.idx, o);
-        if (i2 >= 0 && (mine.idx < 0 || key_better(k2, i2, mine.key, mine.idx))) {
-            mine.key = k2;
-            mine.idx = i2;
-        }
-    }
+    int owner;
+    mine = warp_best(mine, owner);
     if (lane == 0) red[warp] = mine;
     __syncthreads();
     if (warp == 0) {
         const int nw = blockDim.x >> 5;
-        Cand c = (lane < nw) ? red[lane] : Cand{0.f, -1};
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            const float k2 = __shfl_down_sync(0xffffffffu, c.key, o);
-            const int i2 = __shfl_down_sync(0xffffffffu, c.idx, o);
-            if (i2 >= 0 && (c.idx < 0 || key_better(k2, i2, c.key, c.idx))) {
-                c.key = k2;
-                c.idx = i2;
-            }
-        }
+        const Cand c = warp_best((lane < nw) ? red[lane] : Cand{0.f, -1}, owner);
         if (lane == 0) red[32] = c;
     }
     __syncthreads();
@@ -1661,23 +1666,6 @@ __global__ void __launch_bounds__(kNT, c2r_min_blocks<N, T, V>())
     // warps' lists, with one block barrier in between
     __shared__ Cand wl[kNT / 32][16];
     const int lane = tid & 31, warp = tid >> 5;
-    // The lanes' best candidate in selection order (larger key, then smaller
-    // cell index; cell indices are distinct): the largest key by one integer
-    // reduction, the smallest index among the lanes holding it by another.
-    auto warp_best = [&](Cand c, int &owner) {
-        const bool valid = c.idx >= 0;
-        const int ko = valid ? key_ord(c.key) : INT_MIN;
-        const int kmax = __reduce_max_sync(0xffffffffu, ko);
-        const bool tie = valid && ko == kmax;
-        const int imin = __reduce_min_sync(0xffffffffu, tie ? c.idx : INT_MAX);
-        const unsigned win = __ballot_sync(0xffffffffu, tie && c.idx == imin);
-        if (win == 0) {   // no lane holds a candidate
-            owner = 0;
-            return Cand{0.f, -1};
-        }
-        owner = __ffs(win) - 1;
-        return Cand{__shfl_sync(0xffffffffu, c.key, owner), imin};
-    };
     if (__any_sync(0xffffffffu, top.i[0] != INT_MAX)) {
         for (int r = 0; r < nsel; ++r) {
             int owner;
