@@ -242,7 +242,7 @@ def run_profile_case(args):
     from megadock_b200 import FFTProcess, Job, rotation_matrices
     with tempfile.TemporaryDirectory() as tmp:
         rp, lp = make_inputs(tmp)
-        job = Job(["-R", rp, "-L", lp, "-F", str(N_FFT), "-t", str(T_POSES), "-D", "-o",
+        job = Job(["-R", rp, "-L", lp, "-F", str(args.fft or N_FFT), "-t", str(T_POSES), "-D", "-o",
                    os.path.join(tmp, "p.out")])
         mats = rotation_matrices(job.rotation_angles()[:args.profile_case])
         fp = FFTProcess(0)
@@ -520,6 +520,8 @@ def main():
                          "adjoint: forward + LSE adjoint at 96^3, 3,600 rotations; fit: one ranking-loss gradient "
                          "evaluation over 32 planted pairs, 54,000 rotations each")
     ap.add_argument("--fit-pairs", type=int, default=32)
+    ap.add_argument("--fft", type=int, default=0, metavar="N",
+                    help="FFT edge of --profile-case (default 128; the bench pair fits every built size)")
     ap.add_argument("--profile-case", type=int, default=0, metavar="R",
                     help="run R rotations of the batched form once (for ncu captures) and exit")
     ap.add_argument("--profile-aux", action="store_true",

@@ -120,6 +120,7 @@ struct md_ctx {
     int lanes = kLanes;   // work sets / capture streams the batched graph alternates over (1 or 2)
     int cap = 0, cap_t = 0, cap_na = 0;
     WorkSet::Sizes have{};           // bytes held by each work-set buffer
+    int sets = 0;                    // work sets allocated (1 or kLanes)
     WorkSet ws[kLanes];
     char *d_scratch = nullptr;   // scratch of the adjoint and pose-scoring calls (grows to the largest call)
     size_t scratch_cap = 0;

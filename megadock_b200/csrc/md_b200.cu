@@ -61,19 +61,23 @@ void release_work(md_ctx *c) {
     c->d_scratch = nullptr;
     c->scratch_cap = 0;
     c->cap = c->cap_t = c->cap_na = 0;
+    c->sets = 0;
     c->have = WorkSet::Sizes{};
 }
 
-// Work sets holding at least `z` bytes per buffer.
-int ensure_bytes(md_ctx *ctx, const WorkSet::Sizes &z) {
-    bool ok = true;
+// At least `nsets` work sets holding at least `z` bytes per buffer (only the
+// batched graph with two launch groups in flight and the pairs runner use the
+// second set, so one launch group in flight holds one set on the device).
+int ensure_bytes(md_ctx *ctx, const WorkSet::Sizes &z, int nsets) {
+    bool ok = ctx->sets >= nsets;
     for (int k = 0; k < WorkSet::kBufs; ++k) ok = ok && z.b[k] <= ctx->have.b[k];
     if (ok) return MD_OK;
     WorkSet::Sizes m = ctx->have;
     for (int k = 0; k < WorkSet::kBufs; ++k) m.b[k] = std::max(m.b[k], z.b[k]);
     const int cap = ctx->cap, t = ctx->cap_t, na = ctx->cap_na;
     release_work(ctx);
-    for (auto &w : ctx->ws) MD_CUDA(w.allocate(m));
+    for (int k = 0; k < nsets; ++k) MD_CUDA(ctx->ws[k].allocate(m));
+    ctx->sets = nsets;
     ctx->have = m;
     ctx->cap = cap;
     ctx->cap_t = t;
@@ -81,13 +85,13 @@ int ensure_bytes(md_ctx *ctx, const WorkSet::Sizes &z) {
     return MD_OK;
 }
 
-// Work sets for launch groups of `cap` rotations with t poses each.
-int ensure_work(md_ctx *ctx, int cap, int t) {
-    if (cap <= ctx->cap && t <= ctx->cap_t && ctx->na <= ctx->cap_na) return MD_OK;
+// `nsets` work sets for launch groups of `cap` rotations with t poses each.
+int ensure_work(md_ctx *ctx, int cap, int t, int nsets = 1) {
+    if (cap <= ctx->cap && t <= ctx->cap_t && ctx->na <= ctx->cap_na && nsets <= ctx->sets) return MD_OK;
     cap = std::max({cap, ctx->cap, 1});
     t = std::max({t, ctx->cap_t, 1});
     const int na = std::max({ctx->na, ctx->cap_na, 1});
-    int rc = ensure_bytes(ctx, WorkSet::need(cap, ctx->N, t, na));
+    int rc = ensure_bytes(ctx, WorkSet::need(cap, ctx->N, t, na), nsets);
     if (rc) return rc;
     ctx->cap = cap;
     ctx->cap_t = t;
@@ -136,7 +140,7 @@ int check_ready(md_ctx *ctx) {
 // The rotation loop of one md_dock call on device buffers.
 int run_dock(md_ctx *ctx, const float *d_rot, int first_rot, int n_rot, int t, DevPose *d_pose) {
     const int B = std::max(1, std::min(ctx->batch, n_rot));
-    int rc = ensure_work(ctx, B, t);
+    int rc = ensure_work(ctx, B, t, B == 1 ? 1 : ctx->lanes);
     if (rc) return rc;
     if (B == 1) {
         // plain form: one rotation per fused pipeline, launched back to back
@@ -662,7 +666,7 @@ int md_dock_pairs(md_ctx *runner, md_ctx *const *pairs, int npairs, const float 
         key.insert(key.end(), {(uintptr_t)c->uid, (uintptr_t)c->gen, (uintptr_t)d_rotmat[p], (uintptr_t)n_rot[p],
                                (uintptr_t)d_out[p], (uintptr_t)B, (uintptr_t)c->na, (uintptr_t)c->N});
     }
-    int rc = ensure_bytes(ctx, z);
+    int rc = ensure_bytes(ctx, z, kLanes);
     if (rc) return rc;
     auto it = ctx->pair_graphs.find(key);
     if (it == ctx->pair_graphs.end()) {
