@@ -166,6 +166,9 @@ __global__ void k_pose_terms(int ng, int n, const int4 *__restrict__ tem, const 
         const size_t rxc = ng2 * (size_t)(l + tc.x - ng), lxc = ng2 * (size_t)l;
         for (int m = ma; m < mb; ++m) {
             const size_t ryc = rxc + (size_t)ng * (m + tc.y - ng), lyc = lxc + (size_t)ng * m;
+            // unrolled so that the loads of several cells are in flight
+            // while the sums, whose order is fixed, run one cell at a time
+#pragma unroll 8
             for (int k = na; k < nb; ++k) {
                 const size_t rzc = ryc + (size_t)(tc.z + k - ng), lzc = lyc + k;
                 const float a = __ldg(&rec_rpsc[rzc]), b = __ldg(&rec_r[rzc]), c = __ldg(&rec_i[rzc]);

@@ -328,13 +328,16 @@ struct Sized {
         any_fwd<0>(s, nb, L, G, w.vbits, w.qlist, w.qcount, nullptr, nullptr, w.A, nullptr, nullptr);
         if (ev) cudaEventRecord(ev[2], s);
         if (c->tile == 16 && xline_fold_ok<N>())
-            k_xline_fold<N, 16><<<dim3(NH * ((N + 15) / 16), nb), 256, smem_xline<16>(), s>>>(G, w.A, c->d_Rh, w.G);
+            k_xline_fold<N, 16><<<xline_grid<N>(NH * ((N + 15) / 16), nb), 256, smem_xline<16>(), s>>>(G, w.A, c->d_Rh,
+                                                                                                      w.G);
         else if (c->tile == 16)
-            k_xline_herm<N, 16><<<dim3(NH * ((N + 15) / 16), nb), 256, smem_xline<16>(), s>>>(G, w.A, c->d_Rh, w.G);
+            k_xline_herm<N, 16><<<xline_grid<N>(NH * ((N + 15) / 16), nb), 256, smem_xline<16>(), s>>>(G, w.A, c->d_Rh,
+                                                                                                      w.G);
         else if (c->tile == 8)
-            k_xline_herm<N, 8><<<dim3(NH * ((N + 7) / 8), nb), 128, smem_xline<8>(), s>>>(G, w.A, c->d_Rh, w.G);
+            k_xline_herm<N, 8><<<xline_grid<N>(NH * ((N + 7) / 8), nb), 128, smem_xline<8>(), s>>>(G, w.A, c->d_Rh, w.G);
         else
-            k_xline_herm<N, 32><<<dim3(NH * ((N + 31) / 32), nb), 512, smem_xline<32>(), s>>>(G, w.A, c->d_Rh, w.G);
+            k_xline_herm<N, 32><<<xline_grid<N>(NH * ((N + 31) / 32), nb), 512, smem_xline<32>(), s>>>(G, w.A, c->d_Rh,
+                                                                                                      w.G);
         if (ev) cudaEventRecord(ev[3], s);
         plane_topt(s, G, w.G, nb, t, nf3f, w.cand, c->plan);
         if (ev) cudaEventRecord(ev[4], s);

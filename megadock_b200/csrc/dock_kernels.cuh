@@ -856,6 +856,31 @@ constexpr bool xline_tw_smem() {
     return N == 128;
 }
 
+// Block order of the x-line kernels.  Every launch-group rotation reads the
+// same receptor spectrum tiles, which stay in L2 across the launch while the
+// spectrum fits (16 MiB at N = 128); above N = 224 it does not (8 N^3 bytes,
+// 134 MB at N = 256), so the rotation becomes the fastest-varying block index
+// and the launch's rotations read each (ky, kz-tile) of R^ back to back from
+// L2 instead of streaming all of it from HBM once per rotation.
+template <int N>
+constexpr bool xline_rot_fast() {
+    return N > 224;
+}
+template <int N>
+__device__ __forceinline__ void xline_block(int &tile_id, int &b) {
+    if constexpr (xline_rot_fast<N>()) {
+        tile_id = blockIdx.y;
+        b = blockIdx.x;
+    } else {
+        tile_id = blockIdx.x;
+        b = blockIdx.y;
+    }
+}
+template <int N>
+inline dim3 xline_grid(int tiles, int nb) {
+    return xline_rot_fast<N>() ? dim3(nb, tiles) : dim3(tiles, nb);
+}
+
 // Shared memory of k_xline_herm: the own and mirror tiles, and the twiddle
 // table where xline_tw_smem<N>().
 template <int N, int LT>
@@ -884,11 +909,12 @@ __global__ void __launch_bounds__(16 * LT, xline_occ<N>() / LT)
         else return __ldg(&G.tw[j]);
     };
     const int lane = threadIdx.x % LT;
-    const int ky = blockIdx.x / TILES;
-    const int kz = (blockIdx.x % TILES) * LT + lane;
+    int tile_id, b;
+    xline_block<N>(tile_id, b);
+    const int ky = tile_id / TILES;
+    const int kz = (tile_id % TILES) * LT + lane;
     const bool ok = kz < N;
     const int kzm = (N - kz) % N;
-    const int b = blockIdx.y;
     const float2 *Ab = A + (size_t)b * NG * N * N;
     float2 *Gb = Gh + (size_t)b * N * NH * N;
     const int passes = (ky == 0) ? 2 : 1;
@@ -1059,11 +1085,12 @@ __global__ void __launch_bounds__(16 * LT, xline_fold_occ<N>() / LT)
         else return __ldg(&G.tw[j]);
     };
     const int lane = threadIdx.x % LT;
-    const int ky = blockIdx.x / TILES;
-    const int kz = (blockIdx.x % TILES) * LT + lane;
+    int tile_id, b;
+    xline_block<N>(tile_id, b);
+    const int ky = tile_id / TILES;
+    const int kz = (tile_id % TILES) * LT + lane;
     const bool ok = kz < N;
     const int kzm = (N - kz) % N;
-    const int b = blockIdx.y;
     const float2 *Ab = A + (size_t)b * NG * N * N;
     float2 *Gb = Gh + (size_t)b * N * NH * N;
     const int passes = (ky == 0) ? 2 : 1;
