@@ -142,62 +142,110 @@ __global__ void k_pose_dot(int N, int ng, const float *__restrict__ recr, const 
     }
 }
 
-// Score terms of one pose per thread for the detail output
+// Score terms of one pose per warp for the detail output
 // (src/docking.cpp:618-660, :733-812): the ligand cell l of the pose's
 // voxel grid meets receptor cell l + tem - ng on each axis, with
 // tem = (3 ng - t) mod 2 ng, over the same l, m, n ranges and in the same
 // order as the reference, every product rounded before it is added (no
 // FMA), so the float sums are the reference's.  terms[9 p ..]: direct sums of
 // rPSC, ELEC and ACE products, then rPSC+, rPSC-, ELEC+, ELEC-, ACE+, ACE-.
-__global__ void k_pose_terms(int ng, int n, const int4 *__restrict__ tem, const float *__restrict__ rec_r,
-                             const float *__restrict__ rec_rpsc, const float *__restrict__ rec_i,
-                             const float *__restrict__ vr, const float *__restrict__ vi, float *__restrict__ terms) {
-    const int p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= n) return;
+// The sums are one sequential chain per pose, so one lane adds them; the
+// warp's lanes load the next (l, m) row's z segment of the five grids
+// (coalesced) while that lane adds the current row's terms from shared
+// memory, so the loads' latency overlaps the chain instead of stalling it.
+constexpr int kPoseTermWarps = 4;      // poses per CTA
+constexpr int kPoseTermMaxNg = 256;    // longest z segment a row stages
+__global__ void __launch_bounds__(32 * kPoseTermWarps)
+    k_pose_terms(int ng, int n, const int4 *__restrict__ tem, const float *__restrict__ rec_r,
+                 const float *__restrict__ rec_rpsc, const float *__restrict__ rec_i, const float *__restrict__ vr,
+                 const float *__restrict__ vi, float *__restrict__ terms) {
+    constexpr int PER = kPoseTermMaxNg / 32;
+    __shared__ float stage[kPoseTermWarps][5][kPoseTermMaxNg];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int p = blockIdx.x * kPoseTermWarps + warp;
+    if (p >= n) return;   // whole warps only
     const size_t ng2 = (size_t)ng * ng, ng3 = ng2 * ng;
     const int4 tc = tem[p];
     const int la = tc.x < ng ? ng - tc.x : 0, lb = tc.x < ng ? ng : 2 * ng - tc.x;
     const int ma = tc.y < ng ? ng - tc.y : 0, mb = tc.y < ng ? ng : 2 * ng - tc.y;
     const int na = tc.z < ng ? ng - tc.z : 0, nb = tc.z < ng ? ng : 2 * ng - tc.z;
+    const int len = nb - na, per_l = mb - ma;
+    const int rows = (len > 0 && per_l > 0 && lb > la) ? (lb - la) * per_l : 0;
     const float *lr = vr + (size_t)p * ng3, *li = vi + (size_t)p * ng3;
+    float (*st)[kPoseTermMaxNg] = stage[warp];
+    float nx[5][PER];
+    // row r = (l, m) in the reference's order: l outer, m inner
+    auto fetch = [&](int r) {
+        const int l = la + r / per_l, m = ma + r % per_l;
+        const size_t rz0 = ng2 * (size_t)(l + tc.x - ng) + (size_t)ng * (m + tc.y - ng) + (size_t)(tc.z + na - ng);
+        const size_t lz0 = ng2 * (size_t)l + (size_t)ng * m + na;
+#pragma unroll
+        for (int j = 0; j < PER; ++j) {
+            const int k = lane + 32 * j;
+            if (k < len) {
+                nx[0][j] = __ldg(&rec_rpsc[rz0 + k]);
+                nx[1][j] = __ldg(&rec_r[rz0 + k]);
+                nx[2][j] = __ldg(&rec_i[rz0 + k]);
+                nx[3][j] = __ldg(&lr[lz0 + k]);
+                nx[4][j] = __ldg(&li[lz0 + k]);
+            }
+        }
+    };
+    auto park = [&]() {
+#pragma unroll
+        for (int j = 0; j < PER; ++j) {
+            const int k = lane + 32 * j;
+            if (k < len)
+#pragma unroll
+                for (int a = 0; a < 5; ++a) st[a][k] = nx[a][j];
+        }
+    };
     float s_rpsc = 0.f, s_elec = 0.f, s_ace = 0.f;
     float rp = 0.f, rm = 0.f, ep = 0.f, em = 0.f, ap = 0.f, am = 0.f;
-    for (int l = la; l < lb; ++l) {
-        const size_t rxc = ng2 * (size_t)(l + tc.x - ng), lxc = ng2 * (size_t)l;
-        for (int m = ma; m < mb; ++m) {
-            const size_t ryc = rxc + (size_t)ng * (m + tc.y - ng), lyc = lxc + (size_t)ng * m;
-            // unrolled so that the loads of several cells are in flight
-            // while the sums, whose order is fixed, run one cell at a time
-#pragma unroll 8
-            for (int k = na; k < nb; ++k) {
-                const size_t rzc = ryc + (size_t)(tc.z + k - ng), lzc = lyc + k;
-                const float a = __ldg(&rec_rpsc[rzc]), b = __ldg(&rec_r[rzc]), c = __ldg(&rec_i[rzc]);
-                const float x = __ldg(&lr[lzc]), y = __ldg(&li[lzc]);
+    if (rows > 0) {
+        fetch(0);
+        park();
+        __syncwarp();
+    }
+    for (int r = 0; r < rows; ++r) {
+        if (r + 1 < rows) fetch(r + 1);
+        if (lane == 0) {
+            // the signed sums take each term through a select, not a branch:
+            // the same additions in the same order
+#pragma unroll 4
+            for (int k = 0; k < len; ++k) {
+                const float a = st[0][k], b = st[1][k], c = st[2][k];
+                const float x = st[3][k], y = st[4][k];
                 const float rpsc = __fmul_rn(a, x);
                 const float elec = __fmul_rn(c, y);
                 const float ace = __fmul_rn(__fsub_rn(b, a), x);
                 s_rpsc = __fadd_rn(s_rpsc, rpsc);
                 s_elec = __fadd_rn(s_elec, elec);
                 s_ace = __fadd_rn(s_ace, ace);
-                if (rpsc < 0.f) rm = __fadd_rn(rm, rpsc);
-                else if (rpsc > 0.f) rp = __fadd_rn(rp, rpsc);
-                if (elec < 0.f) em = __fadd_rn(em, elec);
-                else if (elec > 0.f) ep = __fadd_rn(ep, elec);
-                if (ace < 0.f) am = __fadd_rn(am, ace);
-                else if (ace > 0.f) ap = __fadd_rn(ap, ace);
+                rm = rpsc < 0.f ? __fadd_rn(rm, rpsc) : rm;
+                rp = rpsc > 0.f ? __fadd_rn(rp, rpsc) : rp;
+                em = elec < 0.f ? __fadd_rn(em, elec) : em;
+                ep = elec > 0.f ? __fadd_rn(ep, elec) : ep;
+                am = ace < 0.f ? __fadd_rn(am, ace) : am;
+                ap = ace > 0.f ? __fadd_rn(ap, ace) : ap;
             }
         }
+        __syncwarp();
+        if (r + 1 < rows) park();
+        __syncwarp();
     }
-    float *o = terms + 9 * (size_t)p;
-    o[0] = s_rpsc;
-    o[1] = s_elec;
-    o[2] = s_ace;
-    o[3] = rp;
-    o[4] = rm;
-    o[5] = ep;
-    o[6] = em;
-    o[7] = ap;
-    o[8] = am;
+    if (lane == 0) {
+        float *o = terms + 9 * (size_t)p;
+        o[0] = s_rpsc;
+        o[1] = s_elec;
+        o[2] = s_ace;
+        o[3] = rp;
+        o[4] = rm;
+        o[5] = ep;
+        o[6] = em;
+        o[7] = ap;
+        o[8] = am;
+    }
 }
 
 }  // namespace mdb

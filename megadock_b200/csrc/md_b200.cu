@@ -944,6 +944,10 @@ int md_pose_terms(md_ctx *ctx, const float *rec_rpsc, const float *rotmat, int n
             ctx->err = "pose offset outside [0, nf1)";
             return MD_ERR_ARG;
         }
+    if (ng > kPoseTermMaxNg) {
+        ctx->err = "pose terms: grid edge above " + std::to_string(kPoseTermMaxNg);
+        return MD_ERR_SIZE;
+    }
     MD_CUDA(cudaSetDevice(ctx->device));
     const size_t ng3 = (size_t)ng * ng * ng;
     // poses per launch: their voxel grids within about 1 GB
@@ -976,8 +980,9 @@ int md_pose_terms(md_ctx *ctx, const float *rec_rpsc, const float *rotmat, int n
                 launch_voxel_chunk(ctx, d_rot + 9 * (size_t)(p0 + b0), nb, d_vox + ng3 * b0,
                                    d_vox + ng3 * ((size_t)P + b0));
             }
-            k_pose_terms<<<(np + 31) / 32, 32, 0, s>>>(ng, np, d_tem + p0, ctx->d_recv, d_rpsc, ctx->d_recv + ng3,
-                                                      d_vox, d_vox + ng3 * P, d_terms + 9 * (size_t)p0);
+            k_pose_terms<<<(np + kPoseTermWarps - 1) / kPoseTermWarps, 32 * kPoseTermWarps, 0, s>>>(
+                ng, np, d_tem + p0, ctx->d_recv, d_rpsc, ctx->d_recv + ng3, d_vox, d_vox + ng3 * P,
+                d_terms + 9 * (size_t)p0);
         }
         step(cudaGetLastError());
         step(cudaMemcpyAsync(terms, d_terms, sizeof(float) * 9 * n, cudaMemcpyDeviceToHost, s));
