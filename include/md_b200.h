@@ -177,7 +177,8 @@ int md_pose_scores(md_ctx *ctx, const float *rotmat, int n, const md_pose *poses
  * ACE products, then rPSC+, rPSC-, ELEC+, ELEC-, ACE+, ACE-.  rec_rpsc is the
  * receptor's real grid without the ACE term (ng1^3, host); the real grid
  * with it and the electrostatic grid are those given to md_receptor_fft.
- * Sums in the reference's cell order, no FMA: the reference's floats. */
+ * Sums in the reference's cell order, no FMA: the reference's floats.  Grids
+ * up to ng1 = 256 (every built FFT size); larger ones return MD_ERR_SIZE. */
 int md_pose_terms(md_ctx *ctx, const float *rec_rpsc, const float *rotmat, int n, const int *tem3, float *terms);
 
 /* Ligand::rpscace + Ligand::electro (src/ligand.cpp:20-239) of one rotation,
