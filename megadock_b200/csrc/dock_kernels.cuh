@@ -1475,7 +1475,11 @@ __global__ void __launch_bounds__(kNT, c2r_min_blocks<N, T, V>())
         // w^{N/2-k} = -conj(w^k).  The folded rows go back to their own slots
         // (eight values in registers at a time, which keeps the kernel at 40
         // registers without spills) and each row set is then reloaded for its
-        // DFT.  B200, N = 128, 13,824 of the 54,000 rotations at 512 per
+        // DFT; the empty asm statements with a memory clobber keep the
+        // compiler from forwarding those stores to the later loads (which
+        // would hold all sixteen values in registers again).  The item's rows
+        // are its own, so no barrier is needed between the two.
+        // B200, N = 128, 13,824 of the 54,000 rotations at 512 per
         // launch, with the warp-owned z pass above: 274.3 ms per 54,000
         // rotations against 287.7 for the separate fold pass; holding both
         // row sets in registers spilled and took 298.0.

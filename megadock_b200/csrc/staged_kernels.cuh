@@ -301,8 +301,63 @@ __global__ void __launch_bounds__(kNTS)
             });
         }
     };
-    if (floor.idx >= 0) scan(std::true_type{});
-    else scan(std::false_type{});
+    if (floor.idx >= 0) {
+        scan(std::true_type{});
+    } else {
+        // First pass: as in k_plane_c2r, the scores go back over the slots
+        // they came from with each thread's maximum; the largest over the
+        // warps of each warp's nsel-th largest lane maximum bounds this
+        // block's nsel-th best key from below, and only cells at or above it
+        // enter the lists (equal keys still compete on the index there).
+        float tmax = -INFINITY;   // fmaxf drops NaN keys, which are never selected
+        for (int it = tid; it < nc * Q1; it += blockDim.x) {
+            const int c = it % nc, u = it / nc;
+            float2 o[Q2];
+            static_for<0, Q2>([&](auto n2_) {
+                constexpr int n2 = decltype(n2_)::value;
+                o[n2] = S[(u * Q2 + n2) * PS + c];
+            });
+            Dft<Q2, +1>::run(o);
+            static_for<0, Q2>([&](auto k2_) {
+                constexpr int k2 = decltype(k2_)::value;
+                S[(u * Q2 + k2) * PS + c] = o[k2];
+                tmax = fmaxf(tmax, fmaxf(o[k2].x, o[k2].y));
+            });
+        }
+        __shared__ float thr_w[kNTS / 32];
+        {
+            const int lane = tid & 31, warp = tid >> 5;
+            float v = tmax, thw = -INFINITY;
+            for (int r = 0; r < nsel; ++r) {
+                const int vo = key_ord(v);
+                const int mo = __reduce_max_sync(0xffffffffu, vo);
+                if (mo == INT_MIN) {   // every lane NaN: no bound from this warp
+                    thw = NAN;
+                    break;
+                }
+                thw = ord_key(mo);
+                const unsigned holders = __ballot_sync(0xffffffffu, vo == mo);
+                if (lane == __ffs(holders) - 1) v = -INFINITY;
+            }
+            if (lane == 0) thr_w[warp] = thw;
+        }
+        __syncthreads();
+        float thr = thr_w[0];
+        for (int w = 1; w < (int)(blockDim.x >> 5); ++w) thr = fmaxf(thr, thr_w[w]);
+        if (tmax >= thr) {
+            for (int it = tid; it < nc * Q1; it += blockDim.x) {
+                const int c = it % nc, u = it / nc;
+                const int cell0 = base + 2 * u * N + c;
+                static_for<0, Q2>([&](auto k2_) {
+                    constexpr int k2 = decltype(k2_)::value;
+                    constexpr int step = 2 * Q1 * k2 * N;
+                    const float2 sc = S[(u * Q2 + k2) * PS + c];
+                    if (sc.x >= thr) top.template insert<false>(sc.x, cell0 + step, floor);
+                    if (sc.y >= thr) top.template insert<false>(sc.y, cell0 + step + N, floor);
+                });
+            }
+        }
+    }
     // block merge: nsel rounds of the block-wide best list head
     for (int r = 0; r < nsel; ++r) {
         const Cand c = block_best(top.head(), red);
