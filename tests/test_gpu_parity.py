@@ -244,6 +244,39 @@ def test_xline_tiles_bit_identical(built, gpu, pairs):
             assert np.array_equal(a, b), (name, tile)
 
 
+@pytest.mark.parametrize("t", [1, 3, 17])
+def test_n128_register_fold_forms_match_fp64_oracle(built, gpu, pairs, t):
+    """N=128 with 16-line x tiles runs the register-fold x-line kernel and the
+    plane kernel's fold-in-ky-pass form with warp-owned z rows (the bench's
+    launch shape): its records match the FP64 oracle for one (t=1), four
+    (t=3) and two passes of sixteen (t=17) selections per plane, the batched
+    graph equals the plain form bit for bit, and the 32-line tiles (the
+    two-phase fold kernel) agree within the tolerance."""
+    from megadock_b200 import rotation_matrices
+    from oracle import oracle as O
+    job, fp = _setup(pairs, "small", "-F", "128", "-r", "360", "-t", str(t))
+    rr, ri = job.receptor_grids()
+    rhat = O.receptor_spectrum(rr, ri, job.nf1, "fp64")
+    sel = np.array([0, 131, 287])
+    mats_all = rotation_matrices(job.rotation_angles()[:20])
+    fp.set_tile(16)
+    plain = fp.cuda_fft(mats_all, t=t).copy()
+    fp.set_batch(8)
+    batched = fp.cuda_fft(mats_all, t=t).copy()
+    assert np.array_equal(plain, batched)
+    fp.set_tile(32)
+    other = fp.cuda_fft(mats_all, t=t).copy()
+    s0, s1 = plain["score"].astype(np.float64), other["score"].astype(np.float64)
+    assert np.all(np.abs(s1 - s0) <= 2 * (RTOL * np.abs(s0) + ATOL))
+    fp.set_tile(16)
+    mats = rotation_matrices(job.rotation_angles()[sel])
+    got = fp.cuda_fft(mats, t=t).copy()
+    for n, r in enumerate(sel):
+        g = got[n * t:(n + 1) * t].copy()
+        g["rot"] = r
+        _check_rotation(g, rhat, job, r, t, mats[n])
+
+
 def test_release_work_then_dock_again(built, gpu, pairs):
     """md_release_work frees the launch groups' buffers and graphs; the next
     call allocates them again (at another launch shape too) and returns the
