@@ -90,3 +90,28 @@ def test_cli_automatic_size_above_224(built, gpu, pairs, tmp_path):
     for n in range(1, len(b) - 1):
         if gaps[n - 1] > 0.05 and gaps[n] > 0.05:
             assert tuple(np.round(b[n, :6], 6)) in ours_set, b[n]
+
+
+@needs_ref
+def test_cli_large_receptor_automatic_size(built, gpu, tmp_path):
+    """A 2,000-residue synthetic receptor with a 250-residue ligand, the grid
+    size chosen automatically from the reference's table (no -F): the command
+    line docks it and writes the reference's .out."""
+    from megadock_b200 import _native, synth
+    from oracle.ref import REF_BIN
+    rp, lp = synth.write_pair(str(tmp_path), 2000, 250, 7, stem="big")
+    flags = ["-R", rp, "-L", lp, "-r", "24", "-t", "2", "-N", "40"]
+    ours, theirs = tmp_path / "ours.out", tmp_path / "ref.out"
+    r1 = subprocess.run([str(_native.CLI_PATH), *flags, "-o", str(ours)], capture_output=True, text=True)
+    assert r1.returncode == 0, r1.stderr
+    r2 = subprocess.run([str(REF_BIN), *flags, "-o", str(theirs)], capture_output=True, text=True)
+    assert r2.returncode == 0
+    h1, a = _parse(ours)
+    h2, b = _parse(theirs)
+    assert h1 == h2
+    np.testing.assert_allclose(a[:, 6], b[:, 6], rtol=1e-4, atol=0.011)
+    ours_set = {tuple(np.round(x[:6], 6)) for x in a}
+    gaps = np.abs(np.diff(b[:, 6]))
+    for n in range(1, len(b) - 1):
+        if gaps[n - 1] > 0.05 and gaps[n] > 0.05:
+            assert tuple(np.round(b[n, :6], 6)) in ours_set, b[n]
