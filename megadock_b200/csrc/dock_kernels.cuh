@@ -753,7 +753,7 @@ __global__ void __launch_bounds__(kNT1B, fwd_cb_fits<N>() ? 2 : 1)
                 constexpr int m = decltype(m_)::value;
                 if constexpr (PR) {
                     if constexpr (m < R1 / 4 || m >= 3 * R1 / 4) {
-                        v[m] = make_float2(0.f, 0.f);
+                        v[m] = make_float2(-0.f, -0.f);
                     } else {
                         v[m] = Z[(t + R2 * (m - R1 / 4)) * PZ + cb + c];   // row n - OFF, n = t + R2 m
                     }
@@ -938,7 +938,7 @@ __global__ void __launch_bounds__(16 * LT, xline_occ<N>() / LT)
                 constexpr int mm = decltype(m_)::value;
                 const int pp = t + R2 * mm - OFF;   // spectrum plane of x = t + R2 mm, if any
                 if constexpr (PR && (mm < R1 / 4 || mm >= 3 * R1 / 4)) {
-                    v1[r][mm] = make_float2(0.f, 0.f);
+                    v1[r][mm] = make_float2(-0.f, -0.f);
                 } else if constexpr (PR) {
                     v1[r][mm] = live ? Ab[((size_t)pp * N + row) * N + col] : make_float2(0.f, 0.f);
                 } else {
@@ -1113,7 +1113,7 @@ __global__ void __launch_bounds__(16 * LT, xline_fold_occ<N>() / LT)
                 constexpr int mm = decltype(m_)::value;
                 const int pp = t + F2 * mm - OFF;   // spectrum plane of x = t + F2 mm, if any
                 if constexpr (PR && (mm < F1 / 4 || mm >= 3 * F1 / 4)) {
-                    v1[r][mm] = make_float2(0.f, 0.f);
+                    v1[r][mm] = make_float2(-0.f, -0.f);
                 } else if constexpr (PR) {
                     v1[r][mm] = live ? Ab[((size_t)pp * N + row) * N + col] : make_float2(0.f, 0.f);
                 } else {

@@ -13,7 +13,10 @@
 //
 // Zero padding: docking grids carry data only in the middle half of each axis
 // ([N/4, 3N/4)).  With R1 % 4 == 0 the pruned phase 1 loads exactly
-// m in [R1/4, 3R1/4) for every t and skips the other (zero) inputs.  When
+// m in [R1/4, 3R1/4) for every t and skips the other (zero) inputs.  The
+// skipped inputs are -0: x + (-0) = x and (-0) - x = -x hold for every x, so
+// the compiler drops those adds from the codelet (with +0 it may not: +0 + -0
+// is +0); the outputs are the same bits (B200, N = 128: identical records).  When
 // N/2 is odd (N % 4 == 2) the data sit at [floor(N/4), floor(N/4) + N/2) and no
 // split prunes evenly: those sizes run the unpruned phase 1 over explicit zeros
 // (prune_ok<N>() false).
@@ -334,7 +337,7 @@ __device__ __forceinline__ void fft_phase1(float2 *b, int es, int t, const float
     static_for<0, R1>([&](auto m_) {
         constexpr int m = decltype(m_)::value;
         if constexpr (PRUNE && (m < R1 / 4 || m >= 3 * R1 / 4)) {
-            v[m] = make_float2(0.f, 0.f);
+            v[m] = make_float2(-0.f, -0.f);
         } else {
             v[m] = b[(t + R2 * m) * es];
         }
