@@ -304,11 +304,11 @@ __global__ void __launch_bounds__(kNTS)
     if (floor.idx >= 0) {
         scan(std::true_type{});
     } else {
-        // First pass: as in k_plane_c2r, the scores go back over the slots
-        // they came from with each thread's maximum; the largest over the
-        // warps of each warp's nsel-th largest lane maximum bounds this
-        // block's nsel-th best key from below, and only cells at or above it
-        // enter the lists (equal keys still compete on the index there).
+        // First pass: as in k_plane_c2r, each thread keeps its maximum; the
+        // largest over the warps of each warp's nsel-th largest lane maximum
+        // bounds this block's nsel-th best key from below, and only the
+        // threads at or above it recompute their items and enter those cells
+        // in the lists (equal keys still compete on the index there).
         float tmax = -INFINITY;   // fmaxf drops NaN keys, which are never selected
         for (int it = tid; it < nc * Q1; it += blockDim.x) {
             const int c = it % nc, u = it / nc;
@@ -320,7 +320,6 @@ __global__ void __launch_bounds__(kNTS)
             Dft<Q2, +1>::run(o);
             static_for<0, Q2>([&](auto k2_) {
                 constexpr int k2 = decltype(k2_)::value;
-                S[(u * Q2 + k2) * PS + c] = o[k2];
                 tmax = fmaxf(tmax, fmaxf(o[k2].x, o[k2].y));
             });
         }
@@ -348,10 +347,16 @@ __global__ void __launch_bounds__(kNTS)
             for (int it = tid; it < nc * Q1; it += blockDim.x) {
                 const int c = it % nc, u = it / nc;
                 const int cell0 = base + 2 * u * N + c;
+                float2 o[Q2];
+                static_for<0, Q2>([&](auto n2_) {
+                    constexpr int n2 = decltype(n2_)::value;
+                    o[n2] = S[(u * Q2 + n2) * PS + c];
+                });
+                Dft<Q2, +1>::run(o);
                 static_for<0, Q2>([&](auto k2_) {
                     constexpr int k2 = decltype(k2_)::value;
                     constexpr int step = 2 * Q1 * k2 * N;
-                    const float2 sc = S[(u * Q2 + k2) * PS + c];
+                    const float2 sc = o[k2];
                     if (sc.x >= thr) top.template insert<false>(sc.x, cell0 + step, floor);
                     if (sc.y >= thr) top.template insert<false>(sc.y, cell0 + step + N, floor);
                 });
