@@ -327,10 +327,16 @@ struct Sized {
         if (ev) cudaEventRecord(ev[1], s);
         any_fwd<0>(s, nb, L, G, w.vbits, w.qlist, w.qcount, nullptr, nullptr, w.A, nullptr, nullptr);
         if (ev) cudaEventRecord(ev[2], s);
-        if (c->tile == 16 && xline_fold_ok<N>())
-            k_xline_fold<N, 16><<<xline_grid<N>(NH * ((N + 15) / 16), nb), 256, smem_xline<16>(), s>>>(G, w.A, c->d_Rh,
-                                                                                                      w.G);
-        else if (c->tile == 16)
+        bool folded = false;   // the register-fold form, instantiated only where it is used
+        if constexpr (xline_fold_ok<N>()) {
+            if (c->tile == 16) {
+                k_xline_fold<N, 16><<<xline_grid<N>(NH * ((N + 15) / 16), nb), 256, smem_xline<16>(), s>>>(
+                    G, w.A, c->d_Rh, w.G);
+                folded = true;
+            }
+        }
+        if (folded) {
+        } else if (c->tile == 16)
             k_xline_herm<N, 16><<<xline_grid<N>(NH * ((N + 15) / 16), nb), 256, smem_xline<16>(), s>>>(G, w.A, c->d_Rh,
                                                                                                       w.G);
         else if (c->tile == 8)
@@ -382,6 +388,8 @@ const SizedOps *sized_ops_k(int N);
 const SizedOps *sized_ops_l(int N);
 const SizedOps *sized_ops_m(int N);
 const SizedOps *sized_ops_n(int N);
+const SizedOps *sized_ops_o(int N);
+const SizedOps *sized_ops_p(int N);
 
 inline const SizedOps *sized_ops(int N) {
     if (const SizedOps *o = sized_ops_a(N)) return o;
@@ -397,7 +405,9 @@ inline const SizedOps *sized_ops(int N) {
     if (const SizedOps *o = sized_ops_k(N)) return o;
     if (const SizedOps *o = sized_ops_l(N)) return o;
     if (const SizedOps *o = sized_ops_m(N)) return o;
-    return sized_ops_n(N);
+    if (const SizedOps *o = sized_ops_n(N)) return o;
+    if (const SizedOps *o = sized_ops_o(N)) return o;
+    return sized_ops_p(N);
 }
 
 }  // namespace mdb

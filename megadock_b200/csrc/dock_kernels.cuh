@@ -409,11 +409,23 @@ constexpr bool vox_bits_dyn() {
     return sizeof(VoxShared<NG>) + sizeof(uint32_t) * 2 * NG * VoxShared<NG>::W > 40 * 1024;
 }
 
-// Dynamic shared memory of k_vox_bits: the first charge entry of each cell,
-// then (vox_bits_dyn) the bit planes and the output words.
+// Whether k_vox_bits keeps the first charge entry of each cell in shared
+// memory (an int per cell): where it fits beside the dynamic bit planes in a
+// CTA's 227 KB (ng1 <= 200).  Above, each entry finds out whether it is its
+// cell's first by scanning the plane's earlier entries (a plane holds the
+// charges of a few hundred atoms at most).
+template <int NG>
+constexpr bool vox_first_smem() {
+    return sizeof(int) * NG * NG +
+               (vox_bits_dyn<NG>() ? sizeof(VoxShared<NG>) + sizeof(uint32_t) * 2 * NG * VoxShared<NG>::W : 0) <=
+           226 * 1024;   // a KB left for the kernel's static shared memory
+}
+
+// Dynamic shared memory of k_vox_bits: the first charge entry of each cell
+// (vox_first_smem), then (vox_bits_dyn) the bit planes and the output words.
 template <int NG>
 constexpr size_t vox_bits_smem() {
-    return sizeof(int) * NG * NG +
+    return (vox_first_smem<NG>() ? sizeof(int) * NG * NG : 0) +
            (vox_bits_dyn<NG>() ? sizeof(VoxShared<NG>) + sizeof(uint32_t) * 2 * NG * VoxShared<NG>::W : 0);
 }
 
@@ -426,11 +438,12 @@ __global__ void __launch_bounds__(kNT0)
     constexpr int W = VoxShared<NG>::W;
     constexpr int NBS = NG + 2 * kReach;
     __shared__ int count;
-    extern __shared__ __align__(16) int first[];   // NG * NG (vox_bits_smem)
+    constexpr bool FIRST = vox_first_smem<NG>();
+    extern __shared__ __align__(16) int first[];   // NG * NG where FIRST (vox_bits_smem)
     VoxShared<NG> *vsp;
     uint32_t(*ob)[NG * W];
     if constexpr (vox_bits_dyn<NG>()) {
-        vsp = reinterpret_cast<VoxShared<NG> *>(first + NG * NG);
+        vsp = reinterpret_cast<VoxShared<NG> *>(first + (FIRST ? NG * NG : 0));
         ob = reinterpret_cast<uint32_t(*)[NG * W]>(vsp + 1);
     } else {
         __shared__ VoxShared<NG> vs_static;
@@ -460,7 +473,8 @@ __global__ void __launch_bounds__(kNT0)
         for (int w = tid; w < 3 * NG * W; w += blockDim.x) (&vs.surf[0][0])[w] = 0u;
     }
     for (int w = tid; w < 2 * NG * W; w += blockDim.x) (&ob[0][0])[w] = 0u;
-    for (int c = tid; c < NG * NG; c += blockDim.x) first[c] = 0x7fffffff;
+    if constexpr (FIRST)
+        for (int c = tid; c < NG * NG; c += blockDim.x) first[c] = 0x7fffffff;
     if (tid == 0) count = 0;
     __syncthreads();
     if constexpr (!PREMARKED) {
@@ -481,12 +495,20 @@ __global__ void __launch_bounds__(kNT0)
     // that cell's entries in order
     const int c0 = cstart[(size_t)b * (NG + 1) + p], c1 = cstart[(size_t)b * (NG + 1) + p + 1];
     const int2 *qb = cq + (size_t)b * L.na;
-    for (int e = c0 + tid; e < c1; e += blockDim.x) atomicMin(&first[qb[e].x], e);
-    __syncthreads();
+    if constexpr (FIRST) {
+        for (int e = c0 + tid; e < c1; e += blockDim.x) atomicMin(&first[qb[e].x], e);
+        __syncthreads();
+    }
     int2 *ql = qlist + ((size_t)b * NG + p) * NG * NG;
     for (int e = c0 + tid; e < c1; e += blockDim.x) {
         const int key = qb[e].x;
-        if (first[key] != e) continue;
+        if constexpr (FIRST) {
+            if (first[key] != e) continue;
+        } else {
+            bool later = false;
+            for (int f = c0; f < e && !later; ++f) later = qb[f].x == key;
+            if (later) continue;
+        }
         float acc = 0.f;
         for (int f = e; f < c1; ++f) {
             const int2 v = qb[f];

@@ -318,6 +318,24 @@ MDB_PLAN(300, 20, 15)
 MDB_PLAN(308, 28, 11)
 MDB_PLAN(320, 16, 20)
 MDB_PLAN(400, 20, 20)
+// edges of the default grid table with ng1 in (160, 220] (staged kernels)
+MDB_PLAN(324, 12, 27)
+MDB_PLAN(330, 22, 15)
+MDB_PLAN(336, 16, 21)
+MDB_PLAN(350, 14, 25)
+MDB_PLAN(352, 16, 22)
+MDB_PLAN(360, 20, 18)
+MDB_PLAN(378, 18, 21)
+MDB_PLAN(384, 16, 24)
+MDB_PLAN(392, 28, 14)
+MDB_PLAN(396, 12, 33)
+MDB_PLAN(420, 20, 21)
+MDB_PLAN(432, 24, 18)
+MDB_PLAN(440, 20, 22)
+// their half edges not listed above
+MDB_PLAN(165, 11, 15)
+MDB_PLAN(175, 7, 25)
+MDB_PLAN(189, 7, 27)
 #undef MDB_PLAN
 
 // Whether the first passes of an axis of length N can skip the zero padding

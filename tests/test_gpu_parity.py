@@ -189,6 +189,10 @@ def _check_rotation(got, rhat, job, r, t, m):
     ("small", ("-F", "308", "-r", "24"), 3, 1),
     ("c0", ("-F", "320", "-v", "0.9", "-r", "24"), 3, 2),
     ("c0", ("-F", "400", "-v", "0.75", "-r", "24"), 2, 1),
+    # ng1 of the default table in (160, 220]: odd ng1 (unpruned), pruned, the largest
+    ("c0", ("-F", "330", "-v", "0.9", "-r", "24"), 2, 1),
+    ("c0", ("-F", "384", "-v", "0.8", "-r", "24"), 3, 1),
+    ("c0", ("-F", "440", "-v", "0.7", "-r", "24"), 1, 1),
     ("c0", ("-F", "256", "-b", "2.5", "-e", "0.06", "-r", "24"), 3, 1),
 ])
 def test_dock_matches_fp64_oracle(built, gpu, pairs, name, extra, t, nchk):
@@ -310,7 +314,7 @@ def test_batched_equals_plain(built, gpu, pairs):
 
 @pytest.mark.parametrize("extra", [("-F", "44", "-v", "2.5"), ("-F", "84"), ("-F", "132"), ("-F", "140"),
                                    ("-F", "50", "-v", "2.5"), ("-F", "110"), ("-F", "154"), ("-F", "192"),
-                                   ("-F", "224"), ("-F", "256"), ("-F", "250")])
+                                   ("-F", "224"), ("-F", "256"), ("-F", "250"), ("-F", "440")])
 def test_batched_forms_at_table_sizes(built, gpu, pairs, extra):
     """The 11-smooth sizes: the batched graph (both lane counts, every tile)
     returns the plain form's records bit for bit; the other radix plans agree
