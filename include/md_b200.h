@@ -85,7 +85,8 @@ int md_release_work(md_ctx *ctx);
  * The autotuner (megadock_b200.tune) picks it together with the batch. */
 int md_set_plan(md_ctx *ctx, int plan);
 /* Tile shape of the x-line kernel: 8, 16 or 32 kz lines per CTA (default
- * 32); also picked by the autotuner. */
+ * 32); also picked by the autotuner.  Above FFT edge 450 a 32-line tile no
+ * longer fits a CTA's shared memory and 16-line tiles run for it. */
 int md_set_tile(md_ctx *ctx, int lines);
 /* Launch groups of the batched form in flight at once: 2 (default) alternates
  * them over two work sets and two streams so that one group's kernels overlap

@@ -218,7 +218,7 @@ struct Sized {
         set((const void *)k_xline_rec<N>, smem_xrec());
         set((const void *)k_vox_bits<NG, true>, smem_vox());
         set((const void *)k_vox_bits<NG, false>, smem_vox());
-        set((const void *)k_xline_herm<N, 32>, smem_xline<32>());
+        if constexpr (xline_tile_fits<N, 32>()) set((const void *)k_xline_herm<N, 32>, smem_xline<32>());
         set((const void *)k_xline_herm<N, 16>, smem_xline<16>());
         set((const void *)k_xline_herm<N, 8>, smem_xline<8>());
         if constexpr (xline_fold_ok<N>()) set((const void *)k_xline_fold<N, 16>, smem_xline<16>());
@@ -341,8 +341,11 @@ struct Sized {
                                                                                                       w.G);
         else if (c->tile == 8)
             k_xline_herm<N, 8><<<xline_grid<N>(NH * ((N + 7) / 8), nb), 128, smem_xline<8>(), s>>>(G, w.A, c->d_Rh, w.G);
-        else
+        else if constexpr (xline_tile_fits<N, 32>())
             k_xline_herm<N, 32><<<xline_grid<N>(NH * ((N + 31) / 32), nb), 512, smem_xline<32>(), s>>>(G, w.A, c->d_Rh,
+                                                                                                      w.G);
+        else
+            k_xline_herm<N, 16><<<xline_grid<N>(NH * ((N + 15) / 16), nb), 256, smem_xline<16>(), s>>>(G, w.A, c->d_Rh,
                                                                                                       w.G);
         if (ev) cudaEventRecord(ev[3], s);
         plane_topt(s, G, w.G, nb, t, nf3f, w.cand, c->plan);
@@ -390,6 +393,8 @@ const SizedOps *sized_ops_m(int N);
 const SizedOps *sized_ops_n(int N);
 const SizedOps *sized_ops_o(int N);
 const SizedOps *sized_ops_p(int N);
+const SizedOps *sized_ops_q(int N);
+const SizedOps *sized_ops_r(int N);
 
 inline const SizedOps *sized_ops(int N) {
     if (const SizedOps *o = sized_ops_a(N)) return o;
@@ -407,7 +412,9 @@ inline const SizedOps *sized_ops(int N) {
     if (const SizedOps *o = sized_ops_m(N)) return o;
     if (const SizedOps *o = sized_ops_n(N)) return o;
     if (const SizedOps *o = sized_ops_o(N)) return o;
-    return sized_ops_p(N);
+    if (const SizedOps *o = sized_ops_p(N)) return o;
+    if (const SizedOps *o = sized_ops_q(N)) return o;
+    return sized_ops_r(N);
 }
 
 }  // namespace mdb

@@ -909,6 +909,12 @@ template <int N, int LT>
 constexpr size_t xline_smem() {
     return (size_t)(2 * N * LT + (xline_tw_smem<N>() ? N : 0)) * sizeof(float2);
 }
+// Whether an LT-line tile fits one CTA's 227 KB (32-line tiles stop at N = 450;
+// above, a request for them runs 16-line tiles).
+template <int N, int LT>
+constexpr bool xline_tile_fits() {
+    return xline_smem<N, LT>() <= 227 * 1024;
+}
 
 template <int N, int LT = kLT>
 __global__ void __launch_bounds__(16 * LT, xline_occ<N>() / LT)

@@ -332,10 +332,25 @@ MDB_PLAN(396, 12, 33)
 MDB_PLAN(420, 20, 21)
 MDB_PLAN(432, 24, 18)
 MDB_PLAN(440, 20, 22)
+// ng1 in (220, 256]
+MDB_PLAN(448, 16, 28)
+MDB_PLAN(450, 18, 25)
+MDB_PLAN(462, 22, 21)
+MDB_PLAN(480, 24, 20)
+MDB_PLAN(484, 44, 11)
+MDB_PLAN(486, 18, 27)
+MDB_PLAN(490, 14, 35)
+MDB_PLAN(500, 20, 25)
+MDB_PLAN(504, 24, 21)
+MDB_PLAN(512, 16, 32)
 // their half edges not listed above
 MDB_PLAN(165, 11, 15)
 MDB_PLAN(175, 7, 25)
 MDB_PLAN(189, 7, 27)
+MDB_PLAN(225, 15, 15)
+MDB_PLAN(231, 11, 21)
+MDB_PLAN(243, 9, 27)
+MDB_PLAN(245, 7, 35)
 #undef MDB_PLAN
 
 // Whether the first passes of an axis of length N can skip the zero padding

@@ -249,7 +249,7 @@ int md_set_grid(md_ctx *ctx, int nf1, float grid_width, const float *grid_coord)
     if (!ctx || !grid_coord || !(grid_width > 0.f)) return MD_ERR_ARG;
     if (!size_supported(nf1)) {
         ctx->err = "FFT size " + std::to_string(nf1) +
-                   " has no built kernel set (built: the default grid table's sizes up to 440; -F picks one)";
+                   " has no built kernel set (built: the default grid table's sizes up to 512; -F picks one)";
         return MD_ERR_SIZE;
     }
     MD_CUDA(cudaSetDevice(ctx->device));

@@ -36,22 +36,23 @@ def test_kernel_sizes_built(built):
               162, 168, 176, 180, 192, 196, 198, 200, 210, 216, 220, 224,
               # staged sizes: every 2 ng1 of the default grid table up to ng1 = 160
               240, 242, 250, 252, 256, 264, 270, 280, 288, 294, 300, 308, 320,
-              324, 330, 336, 350, 352, 360, 378, 384, 392, 396, 400, 420, 432, 440):
+              324, 330, 336, 350, 352, 360, 378, 384, 392, 396, 400, 420, 432, 440,
+              448, 450, 462, 480, 484, 486, 490, 500, 504, 512):
         assert lib().md_fft_size_supported(n) == 1
-    for n in (46, 230, 244, 450, 512, 2048):
+    for n in (46, 230, 244, 520, 1024, 2048):
         assert lib().md_fft_size_supported(n) == 0
 
 
 def test_staged_sizes_cover_the_default_table(built):
     """Every FFT edge 2 ng1 of the default (-l 11) grid table with ng1 in
-    (112, 220] has a kernel set, so automatic sizing never stops below 440."""
+    (112, 256] has a kernel set, so automatic sizing never stops below 512."""
     from pathlib import Path
 
     from megadock_b200 import lib
     tables = Path(__file__).resolve().parent.parent / "megadock_b200" / "data" / "fft_tables.tsv"
     row = [l.split("\t")[1].split() for l in tables.read_text().splitlines() if l.split("\t")[0] == "11"][0]
     for ng1 in map(int, row):
-        if 112 < ng1 <= 220:
+        if 112 < ng1 <= 256:
             assert lib().md_fft_size_supported(2 * ng1) == 1, 2 * ng1
 
 

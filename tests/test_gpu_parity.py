@@ -193,6 +193,9 @@ def _check_rotation(got, rhat, job, r, t, m):
     ("c0", ("-F", "330", "-v", "0.9", "-r", "24"), 2, 1),
     ("c0", ("-F", "384", "-v", "0.8", "-r", "24"), 3, 1),
     ("c0", ("-F", "440", "-v", "0.7", "-r", "24"), 1, 1),
+    # ng1 in (220, 256]: odd ng1 (unpruned), 16-line x tiles for a 32-line request, the largest
+    ("c0", ("-F", "486", "-v", "0.6", "-r", "24"), 2, 1),
+    ("c0", ("-F", "512", "-v", "0.6", "-r", "24"), 3, 1),
     ("c0", ("-F", "256", "-b", "2.5", "-e", "0.06", "-r", "24"), 3, 1),
 ])
 def test_dock_matches_fp64_oracle(built, gpu, pairs, name, extra, t, nchk):
